@@ -1,0 +1,153 @@
+/*
+ * libisf -- C ABI of the B200 (sm_100a) incompressible-Schroedinger-flow
+ * (ISF) library.  Every entry point replaces one call of the reference
+ * SchroedingersSmoke.jl API (paths inside the reference project are cited
+ * beside each declaration); a Julia front-end reaches them through `ccall`.
+ *
+ * Conventions
+ *   - Every function returns an int status: ISF_OK (0) or an ISF_ERR_* code;
+ *     isf_last_error() gives the message.  Nothing aborts the process (the
+ *     reference throws a Julia exception at the same places).
+ *   - Arrays are device pointers with the reference's Julia layouts
+ *     (column-major, x fastest):
+ *       psi        4 floats per cell: re psi1, im psi1, re psi2, im psi2
+ *                  (NTuple{2,ComplexF32}, examples/benchmark.jl:20)
+ *       particles  3 floats per slot; a dead slot is (-1,-1,-1)
+ *                  (src/parallel.jl:213-215)
+ *       jetmask    1 byte per cell (Julia Bool array of isjet.(positions))
+ *   - All work is asynchronous on the handle's stream until isf_sync(), like
+ *     GPUArrays' launches (examples/benchmark.jl:66).  A handle is not
+ *     thread-safe; separate handles are independent.
+ *   - Grid sizes: each of nx, ny, nz in {8,12,16,24,32,48,64,96,128,192,256,
+ *     384,512}, nx a multiple of 16, ny*nz a multiple of 16 (ISF_ERR_INVALID
+ *     otherwise); psi pointers 16-byte aligned, complex arrays 8-byte aligned.
+ */
+#ifndef ISF_H
+#define ISF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define ISF_API __attribute__((visibility("default")))
+#else
+#define ISF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ISF_OK = 0,
+    ISF_ERR_INVALID = 1,     /* bad argument or unsupported size */
+    ISF_ERR_CUDA = 2,        /* CUDA runtime error (message has the CUDA text) */
+    ISF_ERR_NOMEM = 3,       /* device allocation failed */
+};
+
+/* jet phase: reference tuple_dot(k, x) = sum(k .+ x) (src/particles.jl:1,15)
+ * or the dot product k . x (examples/matlabport/simple.jl:47,107) */
+enum { ISF_PHASE_REFERENCE_SUM = 0, ISF_PHASE_DOT = 1 };
+
+/* emission: reference ring (src/particles.jl:86-90), nozzle disc, nozzle cylinder */
+enum { ISF_EMIT_RING = 0, ISF_EMIT_DISC = 1, ISF_EMIT_CYLINDER = 2 };
+
+typedef struct isf_handle isf_handle;
+
+/* ISF{ArrayType,UInt32,Float32}(physical_size, dims, hbar, dt) (src/parallel.jl:41) */
+typedef struct isf_params {
+    int32_t grid_res[3];      /* dims (nx, ny, nz) */
+    int32_t physical_size[3]; /* torus size, integers as in src/parallel.jl:12,45 */
+    float hbar;               /* reduced Planck constant */
+    float dt;                 /* time step */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t flags;            /* reserved, must be 0 */
+    void* stream;             /* cudaStream_t to run on, or NULL: the handle makes its own */
+} isf_params;
+
+/* Arguments of one fused time step (the simloop body, examples/benchmark.jl:46-65). */
+typedef struct isf_step_args {
+    int32_t jet;              /* 0: no nozzle (one projection); 1: jet step */
+    int32_t phase_mode;       /* ISF_PHASE_* */
+    float kvec[3];            /* jet_velocity / hbar (examples/benchmark.jl:24) */
+    float omega_t;            /* omega * t of this step (examples/benchmark.jl:58) */
+    float nozzle_cen[3];
+    float nozzle_len;
+    float nozzle_rad;
+    int32_t emit_mode;        /* ISF_EMIT_* */
+    const uint8_t* jetmask;   /* device isjet array, or NULL to evaluate the nozzle analytically */
+    int64_t emit_start;       /* first ring-buffer slot (0-based) of add_particles! */
+    int64_t emit_count;       /* particles emitted this step (0: none) */
+    uint64_t seed;            /* Philox key */
+    uint64_t counter;         /* Philox stream counter (e.g. the step number) */
+} isf_step_args;
+
+/* ---- handle, memory, stream ------------------------------------------- */
+
+/* ISF constructor (src/parallel.jl:41-98): tables and temporaries on the device. */
+ISF_API int isf_create(const isf_params* params, isf_handle** out);
+ISF_API int isf_destroy(isf_handle* h);
+/* Message of the last failed call on h (or of the last failed isf_create when h is NULL). */
+ISF_API const char* isf_last_error(const isf_handle* h);
+/* The stream the handle's work runs on.  Without a caller stream, isf_create
+ * makes a blocking stream, which is ordered with the legacy default stream. */
+ISF_API int isf_get_stream(const isf_handle* h, void** stream);
+/* GPUArrays.synchronize (examples/benchmark.jl:66) */
+ISF_API int isf_sync(isf_handle* h);
+/* Device buffers for psi / particles / masks (the reference's ArrayType(...) uploads, src/parallel.jl:78-97) */
+ISF_API int isf_malloc(isf_handle* h, void** dptr, size_t bytes);
+ISF_API int isf_free(isf_handle* h, void* dptr);
+/* Stream-ordered copies; host memory should be pinned for asynchrony. */
+ISF_API int isf_memcpy_h2d(isf_handle* h, void* dst_dev, const void* src_host, size_t bytes);
+ISF_API int isf_memcpy_d2h(isf_handle* h, void* dst_host, const void* src_dev, size_t bytes);
+/* grid facts: n[3], d[3] (Float32(physical_size ./ grid_res), src/parallel.jl:46) */
+ISF_API int isf_grid_info(const isf_handle* h, int32_t n_out[3], float d_out[3]);
+
+/* ---- operators (exported API of src/parallel.jl:264-266, src/particles.jl:97) */
+
+/* schroedinger_flow!(isf, psi)            src/parallel.jl:176-187 */
+ISF_API int isf_schroedinger_flow(isf_handle* h, float* psi);
+/* psi .= normalize_psi.(psi)             src/parallel.jl:162-165, examples/benchmark.jl:50 */
+ISF_API int isf_normalize_psi(isf_handle* h, float* psi);
+/* pressure_project!(isf, psi)             src/parallel.jl:155-160 */
+ISF_API int isf_pressure_project(isf_handle* h, float* psi);
+/* velocity_one_form!(isf, psi, hbar)      src/parallel.jl:115-122 (into the handle's velocity) */
+ISF_API int isf_velocity_one_form(isf_handle* h, const float* psi, float hbar);
+/* velocity .*= 1 ./ d (staggered sharp)   examples/benchmark.jl:61-63 */
+ISF_API int isf_staggered_sharp(isf_handle* h);
+/* isf.velocity as AoS float3 per cell     src/parallel.jl:14, 66 (copy into a device buffer) */
+ISF_API int isf_get_velocity(isf_handle* h, float* vel_aos_dev);
+ISF_API int isf_set_velocity(isf_handle* h, const float* vel_aos_dev);
+/* isjet.(isf.positions, cen, len, rad)    src/particles.jl:6-10, examples/benchmark.jl:26 */
+ISF_API int isf_isjet(isf_handle* h, uint8_t* jetmask_dev, const float cen[3], float len, float rad);
+/* restrict_velocity!(isf, psi, kvec, isjetarr, omgterm)   src/particles.jl:25-27
+ * jetmask_dev may be NULL: the nozzle (cen, len, rad) is then evaluated per cell. */
+ISF_API int isf_restrict_velocity(isf_handle* h, float* psi, const float kvec[3], const uint8_t* jetmask_dev,
+                          const float cen[3], float len, float rad, float omgterm, int32_t phase_mode);
+/* add_particles!(particles, start:start+count-1, cen, rad)   src/particles.jl:60-94
+ * slots wrap modulo nslots; seeded Philox stream (seed, counter). */
+ISF_API int isf_add_particles(isf_handle* h, float* particles, int64_t nslots, int64_t start, int64_t count,
+                      const float cen[3], float len, float rad, uint64_t seed, uint64_t counter,
+                      int32_t mode);
+/* staggered_advect!(particles, isf)       src/parallel.jl:248-261 (uses the handle's velocity) */
+ISF_API int isf_staggered_advect(isf_handle* h, float* particles, int64_t nparticles);
+/* One fused time step: the simloop body examples/benchmark.jl:46-65. */
+ISF_API int isf_step(isf_handle* h, float* psi, float* particles, int64_t nparticles, const isf_step_args* args);
+
+/* ---- diagnostics (internal stages of the reference, exposed for parity checks) */
+
+/* isf.f from the handle's velocity: div!(isf)   src/parallel.jl:144-152 */
+ISF_API int isf_div(isf_handle* h, float* f_dev);
+/* real part of poisson_solve with isf.f := f   src/parallel.jl:168-174 */
+ISF_API int isf_poisson_solve(isf_handle* h, const float* f_dev, float* q_dev);
+/* in-place 3D complex FFT of interleaved complex64 data, sign -1 forward
+ * (unnormalised), +1 inverse (1/N): the plan_fft! / plan_ifft! of src/parallel.jl:79 */
+ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
+/* clamp events (staggered_velocity index rounded to n+1) and live particles
+ * of the advections since the last reset */
+ISF_API int isf_counters(isf_handle* h, uint64_t out[2], int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ISF_H */

@@ -1,0 +1,261 @@
+"""B200 (sm_100a) incompressible Schroedinger flow -- host-side mirror of the
+SchroedingersSmoke.jl API over the C ABI of libisf (include/isf.h).
+
+Names follow the reference's exports (src/parallel.jl:264-266,
+src/particles.jl:97); Julia's in-place `!` suffix is dropped.  Device arrays
+are torch CUDA tensors with the reference's layouts:
+
+    psi        float32 (nz, ny, nx, 4): re psi1, im psi1, re psi2, im psi2
+    particles  float32 (P, 3); a dead slot is (-1, -1, -1)
+    isjet mask uint8   (nz, ny, nx)
+
+torch only supplies device memory and the stream for event timing; all
+arithmetic runs in libisf's kernels.  Misuse raises ISFError (the reference
+throws a Julia exception).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, PHASE_DOT, PHASE_REFERENCE_SUM, IsfParams,
+                   IsfStepArgs, ISFError, check, f3)
+
+__all__ = [
+    "ISF", "ISFError", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
+    "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
+    "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER",
+]
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ISFError(_lib.ISF_ERR_INVALID, "arrays must be contiguous CUDA tensors")
+    return C.c_void_p(t.data_ptr())
+
+
+class ISF:
+    """ISF{B200Array, UInt32, Float32}(physical_size, dims, hbar, dt)
+    (src/parallel.jl:41-98): grid, d, velocity and the spectral tables live on
+    the device of `device`."""
+
+    def __init__(self, physical_size, dims, hbar, dt, device: int = 0):
+        if not torch.cuda.is_available():
+            raise ISFError(_lib.ISF_ERR_CUDA, "no CUDA device: libisf has no CPU path")
+        self.L = _lib.load()
+        p = IsfParams()
+        p.grid_res[:] = [int(x) for x in dims]
+        p.physical_size[:] = [int(x) for x in physical_size]
+        p.hbar = float(hbar)
+        p.dt = float(dt)
+        p.device = int(device)
+        p.flags = 0
+        p.stream = None
+        h = C.c_void_p()
+        check(self.L.isf_create(C.byref(p), C.byref(h)))
+        self.h = h
+        self.device = torch.device("cuda", int(device))
+        self.grid_res = tuple(int(x) for x in dims)
+        self.physical_size = tuple(int(x) for x in physical_size)
+        d = (C.c_float * 3)()
+        n = (C.c_int32 * 3)()
+        check(self.L.isf_grid_info(h, n, d), h)
+        self.d = tuple(float(x) for x in d)
+        self.hbar = float(torch.tensor(hbar, dtype=torch.float32))
+        self.dt = float(torch.tensor(dt, dtype=torch.float32))
+        s = C.c_void_p()
+        check(self.L.isf_get_stream(h, C.byref(s)), h)
+        self.stream = torch.cuda.ExternalStream(s.value, device=self.device)
+        nx, ny, nz = self.grid_res
+        self.shape = (nz, ny, nx)
+        self.ncells = nx * ny * nz
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.isf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        """GPUArrays.synchronize (examples/benchmark.jl:66)."""
+        check(self.L.isf_sync(self.h), self.h)
+
+    @property
+    def velocity(self) -> torch.Tensor:
+        """isf.velocity as (nz, ny, nx, 3) float32 (src/parallel.jl:14)."""
+        out = torch.empty(self.shape + (3,), dtype=torch.float32, device=self.device)
+        check(self.L.isf_get_velocity(self.h, _ptr(out)), self.h)
+        self.sync()
+        return out
+
+    @velocity.setter
+    def velocity(self, v: torch.Tensor):
+        v = v.to(self.device, torch.float32).contiguous()
+        check(self.L.isf_set_velocity(self.h, _ptr(v)), self.h)
+        self.sync()
+
+    @property
+    def positions(self) -> torch.Tensor:
+        """isf.positions = (i .- 1) .* d as (nz, ny, nx, 3) (src/parallel.jl:75-77)."""
+        nx, ny, nz = self.grid_res
+        ax = [torch.arange(n, device=self.device, dtype=torch.float32) * torch.tensor(dd, dtype=torch.float32)
+              for n, dd in zip((nx, ny, nz), self.d)]
+        z, y, x = torch.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+        return torch.stack([x, y, z], dim=-1).contiguous()
+
+    # ---- diagnostics
+    def div(self) -> torch.Tensor:
+        f = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        check(self.L.isf_div(self.h, _ptr(f)), self.h)
+        return f
+
+    def poisson_solve(self, f: torch.Tensor) -> torch.Tensor:
+        f = f.contiguous()
+        q = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        check(self.L.isf_poisson_solve(self.h, _ptr(f), _ptr(q)), self.h)
+        return q
+
+    def fft3(self, a: torch.Tensor, sign: int = -1) -> torch.Tensor:
+        """In-place 3D complex FFT of a complex64 (nz, ny, nx) tensor."""
+        if a.dtype != torch.complex64:
+            raise ISFError(_lib.ISF_ERR_INVALID, "fft3 wants complex64")
+        check(self.L.isf_fft3(self.h, _ptr(a), int(sign)), self.h)
+        return a
+
+    def counters(self, reset: bool = False):
+        out = (C.c_uint64 * 2)()
+        check(self.L.isf_counters(self.h, out, int(reset)), self.h)
+        return {"clamp_events": int(out[0]), "live": int(out[1])}
+
+    def _psi(self, psi):
+        if psi.dtype != torch.float32 or tuple(psi.shape) != self.shape + (4,):
+            raise ISFError(_lib.ISF_ERR_INVALID, f"psi must be float32 {self.shape + (4,)}")
+        return _ptr(psi)
+
+    def _parts(self, parts):
+        if parts is None:
+            return None, 0
+        if parts.dtype != torch.float32 or parts.dim() != 2 or parts.shape[1] != 3:
+            raise ISFError(_lib.ISF_ERR_INVALID, "particles must be float32 (P, 3)")
+        return _ptr(parts), int(parts.shape[0])
+
+
+def new_psi(isf: ISF, psi1=1.0, psi2=0.01) -> torch.Tensor:
+    """psi = [(psi1, psi2) for every cell] (examples/benchmark.jl:20)."""
+    p = torch.empty(isf.shape + (4,), dtype=torch.float32, device=isf.device)
+    p[..., 0] = complex(psi1).real
+    p[..., 1] = complex(psi1).imag
+    p[..., 2] = complex(psi2).real
+    p[..., 3] = complex(psi2).imag
+    return p
+
+
+def schroedinger_flow(isf: ISF, psi: torch.Tensor) -> torch.Tensor:
+    """schroedinger_flow!(isf, psi) (src/parallel.jl:176-187)."""
+    check(isf.L.isf_schroedinger_flow(isf.h, isf._psi(psi)), isf.h)
+    return psi
+
+
+def normalize_psi(isf: ISF, psi: torch.Tensor) -> torch.Tensor:
+    """psi .= normalize_psi.(psi) (src/parallel.jl:162-165)."""
+    check(isf.L.isf_normalize_psi(isf.h, isf._psi(psi)), isf.h)
+    return psi
+
+
+def pressure_project(isf: ISF, psi: torch.Tensor) -> torch.Tensor:
+    """pressure_project!(isf, psi) (src/parallel.jl:155-160)."""
+    check(isf.L.isf_pressure_project(isf.h, isf._psi(psi)), isf.h)
+    return psi
+
+
+def velocity_one_form(isf: ISF, psi: torch.Tensor, hbar: float = 1.0) -> None:
+    """velocity_one_form!(isf, psi, hbar = 1f0) (src/parallel.jl:115-122)."""
+    check(isf.L.isf_velocity_one_form(isf.h, isf._psi(psi), float(hbar)), isf.h)
+
+
+def staggered_sharp(isf: ISF) -> None:
+    """isf.velocity .*= 1 ./ isf.d (examples/benchmark.jl:61-63)."""
+    check(isf.L.isf_staggered_sharp(isf.h), isf.h)
+
+
+def isjet(isf: ISF, nozzle_cen, nozzle_len, nozzle_rad) -> torch.Tensor:
+    """isjet.(isf.positions, (cen,), (len,), (rad,)) (src/particles.jl:6-10)."""
+    out = torch.empty(isf.shape, dtype=torch.uint8, device=isf.device)
+    check(isf.L.isf_isjet(isf.h, _ptr(out), f3(nozzle_cen), float(nozzle_len), float(nozzle_rad)), isf.h)
+    return out
+
+
+def restrict_velocity(isf: ISF, psi: torch.Tensor, kvec, isjetarr=None, omgterm: float = 0.0, *,
+                      nozzle=None, phase_mode: int = PHASE_REFERENCE_SUM) -> torch.Tensor:
+    """restrict_velocity!(isf, psi, kvec, isjetarr, omgterm) (src/particles.jl:25-27).
+
+    `isjetarr` is the uint8 isjet array, or None with `nozzle=(cen, len, rad)`
+    to evaluate the nozzle per cell.  The default phase is the reference's
+    tuple_dot (sum(kvec .+ pos)); PHASE_DOT gives k . x.
+    """
+    if isjetarr is None and nozzle is None:
+        raise ISFError(_lib.ISF_ERR_INVALID, "restrict_velocity needs isjetarr or nozzle")
+    cen, ln, rad = nozzle if nozzle is not None else ((0.0, 0.0, 0.0), 0.0, 0.0)
+    check(isf.L.isf_restrict_velocity(isf.h, isf._psi(psi), f3(kvec), _ptr(isjetarr), f3(cen), float(ln),
+                                      float(rad), float(omgterm), int(phase_mode)), isf.h)
+    return psi
+
+
+def add_particles(isf: ISF, particles: torch.Tensor, rng, nozzle_cen, nozzle_rad, *, seed: int = 0,
+                  counter: int = 0, mode: int = EMIT_RING, nozzle_len: float = 0.5) -> None:
+    """add_particles!(particles, range, nozzle_cen, nozzle_rad) (src/particles.jl:60-94).
+
+    `rng` is a Python range of 0-based slots (wrapping modulo the slot count).
+    """
+    ptr, P = isf._parts(particles)
+    start, count = int(rng.start), len(rng)
+    check(isf.L.isf_add_particles(isf.h, ptr, P, start, count, f3(nozzle_cen), float(nozzle_len),
+                                  float(nozzle_rad), int(seed), int(counter), int(mode)), isf.h)
+
+
+def staggered_advect(particles: torch.Tensor, isf: ISF) -> torch.Tensor:
+    """staggered_advect!(particles, isf) (src/parallel.jl:248-261)."""
+    ptr, P = isf._parts(particles)
+    check(isf.L.isf_staggered_advect(isf.h, ptr, P), isf.h)
+    return particles
+
+
+def step_args(jet: dict | None = None) -> IsfStepArgs:
+    a = IsfStepArgs()
+    if jet is None:
+        a.jet = 0
+        return a
+    a.jet = 1
+    a.phase_mode = int(jet.get("phase_mode", PHASE_DOT))
+    a.kvec[:] = [float(x) for x in jet["kvec"]]
+    a.omega_t = float(jet["omega_t"])
+    a.nozzle_cen[:] = [float(x) for x in jet["cen"]]
+    a.nozzle_len = float(jet["len"])
+    a.nozzle_rad = float(jet["rad"])
+    a.emit_mode = int(jet.get("emit_mode", EMIT_RING))
+    m = jet.get("jetmask")
+    a.jetmask = None if m is None else m.data_ptr()
+    a.emit_start = int(jet.get("emit_start", 0))
+    a.emit_count = int(jet.get("emit_count", 0))
+    a.seed = int(jet.get("seed", 0))
+    a.counter = int(jet.get("counter", 0))
+    return a
+
+
+def step(isf: ISF, psi: torch.Tensor, particles: torch.Tensor | None = None, jet: dict | None = None) -> None:
+    """One simloop body (examples/benchmark.jl:46-65) as one fused sequence:
+    schroedinger_flow! -> normalize -> pressure_project! -> [add_particles!,
+    restrict_velocity!, pressure_project!] -> velocity_one_form!(hbar) ->
+    staggered sharp -> staggered_advect!."""
+    ptr, P = isf._parts(particles)
+    a = step_args(jet)
+    check(isf.L.isf_step(isf.h, isf._psi(psi), ptr, P, C.byref(a)), isf.h)

@@ -1,0 +1,126 @@
+"""ctypes binding of libisf.so (the C ABI declared in include/isf.h).
+
+The library is the product: if it is missing, or no CUDA device is usable,
+loading fails loudly -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libisf.so")
+
+ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM = 0, 1, 2, 3
+PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
+EMIT_RING, EMIT_DISC, EMIT_CYLINDER = 0, 1, 2
+
+# every exported entry point of include/isf.h
+EXPORTS = (
+    "isf_create", "isf_destroy", "isf_last_error", "isf_get_stream", "isf_sync", "isf_malloc", "isf_free",
+    "isf_memcpy_h2d", "isf_memcpy_d2h", "isf_grid_info", "isf_schroedinger_flow", "isf_normalize_psi",
+    "isf_pressure_project", "isf_velocity_one_form", "isf_staggered_sharp", "isf_get_velocity",
+    "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
+    "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters",
+)
+
+
+class ISFError(RuntimeError):
+    """A libisf call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libisf error {code}: {msg}")
+        self.code = code
+
+
+class IsfParams(C.Structure):
+    _fields_ = [
+        ("grid_res", C.c_int32 * 3),
+        ("physical_size", C.c_int32 * 3),
+        ("hbar", C.c_float),
+        ("dt", C.c_float),
+        ("device", C.c_int32),
+        ("flags", C.c_int32),
+        ("stream", C.c_void_p),
+    ]
+
+
+class IsfStepArgs(C.Structure):
+    _fields_ = [
+        ("jet", C.c_int32),
+        ("phase_mode", C.c_int32),
+        ("kvec", C.c_float * 3),
+        ("omega_t", C.c_float),
+        ("nozzle_cen", C.c_float * 3),
+        ("nozzle_len", C.c_float),
+        ("nozzle_rad", C.c_float),
+        ("emit_mode", C.c_int32),
+        ("jetmask", C.c_void_p),
+        ("emit_start", C.c_int64),
+        ("emit_count", C.c_int64),
+        ("seed", C.c_uint64),
+        ("counter", C.c_uint64),
+    ]
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libisf.so and declare its signatures."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"libisf.so not built ({p}); run schroedingerssmoke.jl_b200/build.py")
+    L = C.CDLL(p)
+    vp, i32, i64, u64, f32, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_float, C.c_size_t
+    fp = C.POINTER(C.c_float)
+    sig = {
+        "isf_create": [C.POINTER(IsfParams), C.POINTER(vp)],
+        "isf_destroy": [vp],
+        "isf_get_stream": [vp, C.POINTER(vp)],
+        "isf_sync": [vp],
+        "isf_malloc": [vp, C.POINTER(vp), sz],
+        "isf_free": [vp, vp],
+        "isf_memcpy_h2d": [vp, vp, vp, sz],
+        "isf_memcpy_d2h": [vp, vp, vp, sz],
+        "isf_grid_info": [vp, C.POINTER(C.c_int32), fp],
+        "isf_schroedinger_flow": [vp, vp],
+        "isf_normalize_psi": [vp, vp],
+        "isf_pressure_project": [vp, vp],
+        "isf_velocity_one_form": [vp, vp, f32],
+        "isf_staggered_sharp": [vp],
+        "isf_get_velocity": [vp, vp],
+        "isf_set_velocity": [vp, vp],
+        "isf_isjet": [vp, vp, fp, f32, f32],
+        "isf_restrict_velocity": [vp, vp, fp, vp, fp, f32, f32, f32, i32],
+        "isf_add_particles": [vp, vp, i64, i64, i64, fp, f32, f32, u64, u64, i32],
+        "isf_staggered_advect": [vp, vp, i64],
+        "isf_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs)],
+        "isf_div": [vp, vp],
+        "isf_poisson_solve": [vp, vp, vp],
+        "isf_fft3": [vp, vp, i32],
+        "isf_counters": [vp, C.POINTER(C.c_uint64), i32],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.isf_last_error.argtypes = [vp]
+    L.isf_last_error.restype = C.c_char_p
+    if path is None:
+        _lib = L
+    return L
+
+
+def check(rc: int, handle=None):
+    if rc != ISF_OK:
+        msg = load().isf_last_error(handle)
+        raise ISFError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])

@@ -1,0 +1,528 @@
+// C ABI of libisf (declared in include/isf.h): the ISF handle, its device
+// tables and temporaries, and the kernel sequences behind each reference
+// operator.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/isf.h"
+#include "isf_launch.h"
+#include "isf_passes.cuh"
+
+using namespace isf;
+
+struct isf_handle {
+    Grid g;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    float2* F = nullptr;     // Poisson spectrum / complex work array, N
+    float* vel = nullptr;    // velocity planes vx | vy | vz, 3N
+    void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
+    unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(isf_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int cuda_fail(isf_handle* h, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorName(e) + ": " + cudaGetErrorString(e);
+    return fail(h, ISF_ERR_CUDA, m);
+}
+
+#define ISF_CHECK_HANDLE(h)                                                  \
+    do {                                                                     \
+        if (!(h)) return fail(nullptr, ISF_ERR_INVALID, "null isf handle");  \
+    } while (0)
+
+#define ISF_CUDA(h, expr, where)                      \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
+    } while (0)
+
+// Make the handle's device current for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// psi is read as float4 (16-byte) and complex work arrays as float2 (8-byte)
+#define ISF_ALIGNED(h, ptr, a, name)                                                        \
+    do {                                                                                    \
+        if (((uintptr_t)(ptr)) % (a) != 0)                                                  \
+            return fail(h, ISF_ERR_INVALID, std::string(name) + " must be " #a "-byte aligned"); \
+    } while (0)
+
+#define ISF_ENTER(h)                                          \
+    ISF_CHECK_HANDLE(h);                                      \
+    DeviceGuard guard_(h->device);                            \
+    if (guard_.err != cudaSuccess) return cuda_fail(h, guard_.err, "cudaSetDevice")
+
+const double kPi = 3.14159265358979323846264338327950288;
+
+bool valid_grid(const int n[3], std::string& why) {
+    for (int a = 0; a < 3; ++a) {
+        if (!supported_len(n[a])) {
+            why = "grid_res[" + std::to_string(a) + "] = " + std::to_string(n[a]) +
+                  " is not one of 8,12,16,24,32,48,64,96,128,192,256,384,512";
+            return false;
+        }
+    }
+    if (n[0] % 16 != 0) {
+        why = "grid_res[0] must be a multiple of 16";
+        return false;
+    }
+    if (((long long)n[1] * n[2]) % 16 != 0) {
+        why = "grid_res[1]*grid_res[2] must be a multiple of 16";
+        return false;
+    }
+    return true;
+}
+
+XArgs xargs(isf_handle* h) {
+    XArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = h->g;
+    a.F = h->F;
+    return a;
+}
+
+YZArgs yzargs(isf_handle* h, void* data, int axis) {
+    YZArgs a;
+    a.g = h->g;
+    a.data = data;
+    a.axis = axis;
+    return a;
+}
+
+// schroedinger_flow! (+ normalize fused into the last pass when norm != 0)
+int run_schroedinger(isf_handle* h, float* psi, bool norm) {
+    XArgs xa = xargs(h);
+    xa.psi = reinterpret_cast<float4*>(psi);
+    ISF_CUDA(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
+    ISF_CUDA(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
+    ISF_CUDA(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");
+    ISF_CUDA(h, launch_yzpass_psi(YZ_INV, yzargs(h, psi, 1), h->stream), "schroedinger y inv");
+    ISF_CUDA(h, launch_xpass(norm ? X_PSI_INV_NORM : X_PSI_INV, xa, h->stream), "schroedinger x inv");
+    return ISF_OK;
+}
+
+// pressure_project! with the optional nozzle restriction fused in front
+int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
+    XArgs xa = xargs(h);
+    xa.psi = reinterpret_cast<float4*>(psi);
+    if (jet) {
+        xa.jet = *jet;
+        xa.use_jet = 1;
+    }
+    ISF_CUDA(h, launch_xpass(X_STENCIL_FWD, xa, h->stream), "projection div + x fwd");
+    ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "projection y fwd");
+    ISF_CUDA(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "projection z fac");
+    ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "projection y inv");
+    ISF_CUDA(h, launch_xpass(X_GAUGE_INV, xa, h->stream), "projection x inv + gauge");
+    return ISF_OK;
+}
+
+JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], float len, float rad, float omgterm,
+                 int mode) {
+    JetArgs j;
+    for (int a = 0; a < 3; ++a) {
+        j.kvec[a] = kvec[a];
+        j.cen[a] = cen[a];
+    }
+    j.len = len;
+    j.rad = rad;
+    j.omgterm = omgterm;
+    j.phase_mode = mode;
+    j.mask = mask;
+    return j;
+}
+
+}  // namespace
+
+extern "C" {
+
+int isf_create(const isf_params* p, isf_handle** out) {
+    if (!p || !out) return fail(nullptr, ISF_ERR_INVALID, "isf_create: null argument");
+    *out = nullptr;
+    std::string why;
+    if (!valid_grid(p->grid_res, why)) return fail(nullptr, ISF_ERR_INVALID, "isf_create: " + why);
+    for (int a = 0; a < 3; ++a)
+        if (p->physical_size[a] <= 0) return fail(nullptr, ISF_ERR_INVALID, "isf_create: physical_size must be > 0");
+    if (!(p->dt > 0.f) || !std::isfinite(p->hbar) || !std::isfinite(p->dt))
+        return fail(nullptr, ISF_ERR_INVALID, "isf_create: hbar and dt must be finite, dt > 0");
+    if (p->flags != 0) return fail(nullptr, ISF_ERR_INVALID, "isf_create: flags must be 0");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "isf_create: cudaGetDeviceCount");
+    if (p->device < 0 || p->device >= ndev) return fail(nullptr, ISF_ERR_INVALID, "isf_create: bad device ordinal");
+
+    isf_handle* h = new isf_handle();
+    h->device = p->device;
+    DeviceGuard guard(h->device);
+    if (guard.err != cudaSuccess) {
+        delete h;
+        return cuda_fail(nullptr, guard.err, "isf_create: cudaSetDevice");
+    }
+    Grid& g = h->g;
+    std::memset(&g, 0, sizeof(g));
+    for (int a = 0; a < 3; ++a) {
+        g.n[a] = p->grid_res[a];
+        g.L[a] = (float)p->physical_size[a];
+        g.d[a] = (float)((double)p->physical_size[a] / (double)p->grid_res[a]);  // parallel.jl:46
+        g.inv_d2[a] = 1.0f / (g.d[a] * g.d[a]);                                  // parallel.jl:150
+        g.dinv[a] = 1.0f / g.d[a];                                                // benchmark.jl:62
+    }
+    g.N = (long long)g.n[0] * g.n[1] * g.n[2];
+    g.hbar = p->hbar;
+    g.dt = p->dt;
+    g.invN = 1.0 / (double)g.N;
+
+    // host tables in double
+    size_t tw_bytes = 0, mt_bytes = 0, s2_bytes = 0;
+    for (int a = 0; a < 3; ++a) {
+        tw_bytes += sizeof(float2) * g.n[a];
+        mt_bytes += sizeof(double2) * g.n[a];
+        s2_bytes += sizeof(double) * g.n[a];
+    }
+    const size_t total = mt_bytes + s2_bytes + tw_bytes;
+    std::string host(total, '\0');
+    double2* mt = reinterpret_cast<double2*>(&host[0]);
+    double* s2 = reinterpret_cast<double*>(&host[mt_bytes]);
+    float2* tw = reinterpret_cast<float2*>(&host[mt_bytes + s2_bytes]);
+    const double fm = -4.0 * kPi * kPi * (double)p->hbar;  // f = -4 pi^2 hbar (parallel.jl:49)
+    size_t off = 0;
+    for (int a = 0; a < 3; ++a) {
+        const int n = g.n[a];
+        for (int k = 0; k < n; ++k) {
+            // fftshift'ed frequency (parallel.jl:58, 62): k' = k for k < n/2, k - n otherwise
+            const double ks = (k < n / 2) ? (double)k : (double)(k - n);
+            const double kk = ks / (double)p->physical_size[a];
+            const double th = fm * kk * kk * (double)p->dt / 2.0;
+            mt[off + k] = make_double2(std::cos(th), std::sin(th));
+            const double s = std::sin(kPi * (double)k / (double)n) / (double)g.d[a];  // parallel.jl:53
+            s2[off + k] = s * s;
+            const long double ang = -2.0L * (long double)kPi * (long double)k / (long double)n;
+            tw[off + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        off += n;
+    }
+
+    auto cleanup = [&](int code, const std::string& msg) {
+        if (h->F) cudaFree(h->F);
+        if (h->vel) cudaFree(h->vel);
+        if (h->tables) cudaFree(h->tables);
+        if (h->counters) cudaFree(h->counters);
+        if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+        delete h;
+        return fail(nullptr, code, msg);
+    };
+    if (p->stream) {
+        h->stream = (cudaStream_t)p->stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&h->stream, cudaStreamDefault);  // orders with the legacy default stream
+        if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: stream: ") + cudaGetErrorString(e));
+        h->own_stream = true;
+    }
+    if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess ||
+        cudaMalloc(&h->vel, sizeof(float) * 3 * g.N) != cudaSuccess ||
+        cudaMalloc(&h->tables, total) != cudaSuccess ||
+        cudaMalloc(&h->counters, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        return cleanup(ISF_ERR_NOMEM, "isf_create: device allocation failed");
+    }
+    e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float) * 3 * g.N);
+    if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
+    char* base = reinterpret_cast<char*>(h->tables);
+    off = 0;
+    for (int a = 0; a < 3; ++a) {
+        g.mtab[a] = reinterpret_cast<const double2*>(base) + off;
+        g.s2[a] = reinterpret_cast<const double*>(base + mt_bytes) + off;
+        g.tw[a] = reinterpret_cast<const float2*>(base + mt_bytes + s2_bytes) + off;
+        off += g.n[a];
+    }
+    *out = h;
+    return ISF_OK;
+}
+
+int isf_destroy(isf_handle* h) {
+    if (!h) return ISF_OK;
+    {
+        DeviceGuard guard(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        cudaFree(h->F);
+        cudaFree(h->vel);
+        cudaFree(h->tables);
+        cudaFree(h->counters);
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+    return ISF_OK;
+}
+
+const char* isf_last_error(const isf_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int isf_sync(isf_handle* h) {
+    ISF_ENTER(h);
+    ISF_CUDA(h, cudaStreamSynchronize(h->stream), "isf_sync");
+    return ISF_OK;
+}
+
+int isf_malloc(isf_handle* h, void** dptr, size_t bytes) {
+    ISF_ENTER(h);
+    if (!dptr) return fail(h, ISF_ERR_INVALID, "isf_malloc: null out pointer");
+    if (cudaMalloc(dptr, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *dptr = nullptr;
+        return fail(h, ISF_ERR_NOMEM, "isf_malloc: cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+    }
+    return ISF_OK;
+}
+
+int isf_free(isf_handle* h, void* dptr) {
+    ISF_ENTER(h);
+    ISF_CUDA(h, cudaStreamSynchronize(h->stream), "isf_free: sync");
+    ISF_CUDA(h, cudaFree(dptr), "isf_free");
+    return ISF_OK;
+}
+
+int isf_memcpy_h2d(isf_handle* h, void* dst, const void* src, size_t bytes) {
+    ISF_ENTER(h);
+    if (bytes == 0) return ISF_OK;
+    if (!dst || !src) return fail(h, ISF_ERR_INVALID, "isf_memcpy_h2d: null pointer");
+    ISF_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream), "isf_memcpy_h2d");
+    return ISF_OK;
+}
+
+int isf_memcpy_d2h(isf_handle* h, void* dst, const void* src, size_t bytes) {
+    ISF_ENTER(h);
+    if (bytes == 0) return ISF_OK;
+    if (!dst || !src) return fail(h, ISF_ERR_INVALID, "isf_memcpy_d2h: null pointer");
+    ISF_CUDA(h, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream), "isf_memcpy_d2h");
+    return ISF_OK;
+}
+
+int isf_get_stream(const isf_handle* h, void** stream) {
+    if (!h || !stream) return fail(nullptr, ISF_ERR_INVALID, "isf_get_stream: null argument");
+    *stream = (void*)h->stream;
+    return ISF_OK;
+}
+
+int isf_grid_info(const isf_handle* h, int32_t n_out[3], float d_out[3]) {
+    if (!h) return fail(nullptr, ISF_ERR_INVALID, "null isf handle");
+    for (int a = 0; a < 3; ++a) {
+        if (n_out) n_out[a] = h->g.n[a];
+        if (d_out) d_out[a] = h->g.d[a];
+    }
+    return ISF_OK;
+}
+
+int isf_schroedinger_flow(isf_handle* h, float* psi) {
+    ISF_ENTER(h);
+    if (!psi) return fail(h, ISF_ERR_INVALID, "isf_schroedinger_flow: null psi");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    return run_schroedinger(h, psi, false);
+}
+
+int isf_normalize_psi(isf_handle* h, float* psi) {
+    ISF_ENTER(h);
+    if (!psi) return fail(h, ISF_ERR_INVALID, "isf_normalize_psi: null psi");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    ISF_CUDA(h, launch_normalize(h->g, reinterpret_cast<float4*>(psi), h->stream), "normalize");
+    return ISF_OK;
+}
+
+int isf_pressure_project(isf_handle* h, float* psi) {
+    ISF_ENTER(h);
+    if (!psi) return fail(h, ISF_ERR_INVALID, "isf_pressure_project: null psi");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    return run_projection(h, psi, nullptr);
+}
+
+int isf_velocity_one_form(isf_handle* h, const float* psi, float hbar) {
+    ISF_ENTER(h);
+    if (!psi) return fail(h, ISF_ERR_INVALID, "isf_velocity_one_form: null psi");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    ISF_CUDA(h, launch_one_form(h->g, reinterpret_cast<const float4*>(psi), h->vel, hbar, 0, h->stream), "one_form");
+    return ISF_OK;
+}
+
+int isf_staggered_sharp(isf_handle* h) {
+    ISF_ENTER(h);
+    ISF_CUDA(h, launch_sharp(h->g, h->vel, h->stream), "staggered_sharp");
+    return ISF_OK;
+}
+
+int isf_get_velocity(isf_handle* h, float* aos) {
+    ISF_ENTER(h);
+    if (!aos) return fail(h, ISF_ERR_INVALID, "isf_get_velocity: null buffer");
+    ISF_CUDA(h, launch_vel_to_aos(h->g, h->vel, aos, h->stream), "get_velocity");
+    return ISF_OK;
+}
+
+int isf_set_velocity(isf_handle* h, const float* aos) {
+    ISF_ENTER(h);
+    if (!aos) return fail(h, ISF_ERR_INVALID, "isf_set_velocity: null buffer");
+    ISF_CUDA(h, launch_vel_from_aos(h->g, aos, h->vel, h->stream), "set_velocity");
+    return ISF_OK;
+}
+
+int isf_isjet(isf_handle* h, uint8_t* mask, const float cen[3], float len, float rad) {
+    ISF_ENTER(h);
+    if (!mask || !cen) return fail(h, ISF_ERR_INVALID, "isf_isjet: null argument");
+    ISF_CUDA(h, launch_isjet(h->g, mask, cen, len, rad, h->stream), "isjet");
+    return ISF_OK;
+}
+
+int isf_restrict_velocity(isf_handle* h, float* psi, const float kvec[3], const uint8_t* mask, const float cen[3],
+                          float len, float rad, float omgterm, int32_t phase_mode) {
+    ISF_ENTER(h);
+    if (!psi || !kvec || (!mask && !cen)) return fail(h, ISF_ERR_INVALID, "isf_restrict_velocity: null argument");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    if (phase_mode != ISF_PHASE_REFERENCE_SUM && phase_mode != ISF_PHASE_DOT)
+        return fail(h, ISF_ERR_INVALID, "isf_restrict_velocity: bad phase_mode");
+    const float zero[3] = {0.f, 0.f, 0.f};
+    JetArgs j = make_jet(kvec, mask, cen ? cen : zero, len, rad, omgterm, phase_mode);
+    ISF_CUDA(h, launch_restrict(h->g, reinterpret_cast<float4*>(psi), j, h->stream), "restrict_velocity");
+    return ISF_OK;
+}
+
+int isf_add_particles(isf_handle* h, float* parts, int64_t nslots, int64_t start, int64_t count, const float cen[3],
+                      float len, float rad, uint64_t seed, uint64_t counter, int32_t mode) {
+    ISF_ENTER(h);
+    if (!parts || !cen) return fail(h, ISF_ERR_INVALID, "isf_add_particles: null argument");
+    if (nslots <= 0 || count < 0 || start < 0) return fail(h, ISF_ERR_INVALID, "isf_add_particles: bad slot range");
+    if (count > nslots) return fail(h, ISF_ERR_INVALID, "isf_add_particles: count exceeds the number of slots");
+    if (mode < ISF_EMIT_RING || mode > ISF_EMIT_CYLINDER) return fail(h, ISF_ERR_INVALID, "isf_add_particles: bad mode");
+    EmitArgs e;
+    for (int a = 0; a < 3; ++a) e.cen[a] = cen[a];
+    e.len = len;
+    e.rad = rad;
+    e.seed = seed;
+    e.counter = counter;
+    e.mode = mode;
+    ISF_CUDA(h, launch_emit(parts, nslots, start % nslots, count, e, h->stream), "add_particles");
+    return ISF_OK;
+}
+
+int isf_staggered_advect(isf_handle* h, float* parts, int64_t np) {
+    ISF_ENTER(h);
+    if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_staggered_advect: bad particles");
+    ISF_CUDA(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "staggered_advect");
+    return ISF_OK;
+}
+
+int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step_args* a) {
+    ISF_ENTER(h);
+    if (!psi || !a) return fail(h, ISF_ERR_INVALID, "isf_step: null argument");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_step: bad particles");
+    if (a->jet) {
+        if (a->phase_mode != ISF_PHASE_REFERENCE_SUM && a->phase_mode != ISF_PHASE_DOT)
+            return fail(h, ISF_ERR_INVALID, "isf_step: bad phase_mode");
+        if (a->emit_count < 0 || a->emit_start < 0 || (a->emit_count > 0 && (np <= 0 || a->emit_count > np)))
+            return fail(h, ISF_ERR_INVALID, "isf_step: bad emission range");
+        if (a->emit_count > 0 && (a->emit_mode < ISF_EMIT_RING || a->emit_mode > ISF_EMIT_CYLINDER))
+            return fail(h, ISF_ERR_INVALID, "isf_step: bad emit_mode");
+    }
+    int rc = run_schroedinger(h, psi, true);  // schroedinger_flow! + normalize_psi
+    if (rc) return rc;
+    rc = run_projection(h, psi, nullptr);     // pressure_project!
+    if (rc) return rc;
+    if (a->jet) {
+        if (a->emit_count > 0) {
+            EmitArgs e;
+            for (int k = 0; k < 3; ++k) e.cen[k] = a->nozzle_cen[k];
+            e.len = a->nozzle_len;
+            e.rad = a->nozzle_rad;
+            e.seed = a->seed;
+            e.counter = a->counter;
+            e.mode = a->emit_mode;
+            ISF_CUDA(h, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, h->stream), "step emit");
+        }
+        JetArgs j = make_jet(a->kvec, a->jetmask, a->nozzle_cen, a->nozzle_len, a->nozzle_rad, a->omega_t,
+                             a->phase_mode);
+        rc = run_projection(h, psi, &j);  // restrict_velocity! + pressure_project!
+        if (rc) return rc;
+    }
+    // velocity_one_form!(isf, psi, isf.hbar) + staggered sharp
+    ISF_CUDA(h, launch_one_form(h->g, reinterpret_cast<const float4*>(psi), h->vel, h->g.hbar, 1, h->stream),
+             "step one_form");
+    if (np > 0) ISF_CUDA(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "step advect");
+    return ISF_OK;
+}
+
+int isf_div(isf_handle* h, float* f) {
+    ISF_ENTER(h);
+    if (!f) return fail(h, ISF_ERR_INVALID, "isf_div: null output");
+    ISF_CUDA(h, launch_div(h->g, h->vel, f, h->stream), "div");
+    return ISF_OK;
+}
+
+int isf_poisson_solve(isf_handle* h, const float* f, float* q) {
+    ISF_ENTER(h);
+    if (!f || !q) return fail(h, ISF_ERR_INVALID, "isf_poisson_solve: null argument");
+    XArgs xa = xargs(h);
+    xa.rin = f;
+    xa.rout = q;
+    ISF_CUDA(h, launch_xpass(X_REAL_FWD, xa, h->stream), "poisson x fwd");
+    ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "poisson y fwd");
+    ISF_CUDA(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "poisson z fac");
+    ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "poisson y inv");
+    ISF_CUDA(h, launch_xpass(X_REAL_INV, xa, h->stream), "poisson x inv");
+    return ISF_OK;
+}
+
+int isf_fft3(isf_handle* h, float* data, int32_t sign) {
+    ISF_ENTER(h);
+    if (!data || (sign != -1 && sign != 1)) return fail(h, ISF_ERR_INVALID, "isf_fft3: bad argument");
+    ISF_ALIGNED(h, data, 8, "data");
+    XArgs xa = xargs(h);
+    xa.F = reinterpret_cast<float2*>(data);
+    if (sign < 0) {
+        ISF_CUDA(h, launch_xpass(X_C_FWD, xa, h->stream), "fft3 x");
+        ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 1), h->stream), "fft3 y");
+        ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 2), h->stream), "fft3 z");
+    } else {
+        ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 2), h->stream), "ifft3 z");
+        ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 1), h->stream), "ifft3 y");
+        ISF_CUDA(h, launch_xpass(X_C_INV, xa, h->stream), "ifft3 x");
+        ISF_CUDA(h, launch_scale_c(h->g, reinterpret_cast<float2*>(data), (float)h->g.invN, h->stream), "ifft3 scale");
+    }
+    return ISF_OK;
+}
+
+int isf_counters(isf_handle* h, uint64_t out[2], int32_t reset) {
+    ISF_ENTER(h);
+    unsigned long long tmp[2] = {0, 0};
+    ISF_CUDA(h, cudaMemcpyAsync(tmp, h->counters, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream), "counters");
+    ISF_CUDA(h, cudaStreamSynchronize(h->stream), "counters sync");
+    if (out) {
+        out[0] = tmp[0];
+        out[1] = tmp[1];
+    }
+    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), h->stream), "counters reset");
+    return ISF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// Shared device helpers for the ISF sm_100a kernels.
+//
+// Layouts in HBM (identical to the reference's Julia arrays, 0-based):
+//   cell index  c = x + nx*(y + ny*z)  (column-major, x fastest)
+//   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
+//               == NTuple{2,ComplexF32} of src/parallel.jl
+//   velocity    three planes vx[N], vy[N], vz[N] (SoA, internal to the handle)
+//   F           float2 per cell: the Poisson spectrum work array
+//   particles   float3 per slot (AoS), dead slot = (-1,-1,-1)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace isf {
+
+struct Grid {
+    int n[3];          // grid_res
+    long long N;       // nx*ny*nz
+    float L[3];        // physical_size (integers in the reference, parallel.jl:12)
+    float d[3];        // Float32(L/n)                      parallel.jl:46
+    float inv_d2[3];   // inv.(d .^ 2f0)                    parallel.jl:150
+    float dinv[3];     // inv.(d)                           benchmark.jl:62
+    float hbar, dt;
+    const float2* tw[3];    // tw[a][j] = exp(-2 pi i j / n[a]) rounded from double
+    const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))
+    const double* s2[3];    // (sin(pi k / n_a) / d_a)^2 in double
+    double invN;            // 1 / N
+};
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float4 cadd(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 csub(float4 a, float4 b) {
+    return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 w) {
+    return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+}
+__device__ __forceinline__ float4 cmul(float4 a, float2 w) {
+    return make_float4(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x, a.z * w.x - a.w * w.y, a.z * w.y + a.w * w.x);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float4 cscale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+// multiply by S*i (S = +1 or -1): (x + iy)(S i) = -S y + i S x
+template <int S>
+__device__ __forceinline__ float2 mul_si(float2 a) {
+    return S < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+template <int S>
+__device__ __forceinline__ float4 mul_si(float4 a) {
+    return S < 0 ? make_float4(a.y, -a.x, a.w, -a.z) : make_float4(-a.y, a.x, -a.w, a.z);
+}
+
+__host__ __device__ __forceinline__ long long cell(const Grid& g, int x, int y, int z) {
+    return (long long)x + (long long)g.n[0] * ((long long)y + (long long)g.n[1] * z);
+}
+
+// Julia `angle(conj(a1)*b1 + conj(a2)*b2)` for psi pairs a, b (parallel.jl:108-111)
+__device__ __forceinline__ float pair_angle(float4 a, float4 b) {
+    // conj(a1)*b1 = (a.x - i a.y)(b.x + i b.y)
+    float re = a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
+    float im = a.x * b.y - a.y * b.x + a.z * b.w - a.w * b.z;
+    return atan2f(im, re);
+}
+
+// particles.jl:6-10, evaluated in float with every operation rounded on its
+// own (no fused multiply-add), as the reference's broadcast over Float32
+// positions does.
+__device__ __forceinline__ bool isjet_f32(float px, float py, float pz, const float* cen, float len, float rad) {
+    float dx = fabsf(__fsub_rn(px, cen[0]));
+    float h = __fdiv_rn(len, 2.0f);
+    float dy = __fsub_rn(py, cen[1]);
+    float dz = __fsub_rn(pz, cen[2]);
+    float s = __fadd_rn(__fmul_rn(dy, dy), __fmul_rn(dz, dz));
+    return (dx <= h) && (s <= __fmul_rn(rad, rad));
+}
+
+struct JetArgs {
+    float kvec[3];
+    float cen[3];
+    float len, rad;
+    float omgterm;
+    int phase_mode;          // 0: reference tuple_dot = sum(k .+ x); 1: k . x
+    const uint8_t* mask;     // optional precomputed isjet array (N bytes) or null
+};
+
+// restrict_kernel (particles.jl:12-20) for cell (x,y,z); returns true if
+// the cell is a nozzle cell and v was replaced.
+__device__ __forceinline__ bool restrict_cell(const Grid& g, const JetArgs& j, int x, int y, int z, long long c,
+                                              float4& v) {
+    const float px = __fmul_rn((float)x, g.d[0]);
+    const float py = __fmul_rn((float)y, g.d[1]);
+    const float pz = __fmul_rn((float)z, g.d[2]);
+    bool jet = j.mask ? (j.mask[c] != 0) : isjet_f32(px, py, pz, j.cen, j.len, j.rad);
+    if (!jet) return false;
+    float ph;
+    if (j.phase_mode == 0)
+        ph = __fadd_rn(__fadd_rn(__fadd_rn(j.kvec[0], px), __fadd_rn(j.kvec[1], py)), __fadd_rn(j.kvec[2], pz));
+    else
+        ph = j.kvec[0] * px + j.kvec[1] * py + j.kvec[2] * pz;
+    ph = ph - j.omgterm;
+    float s, co;
+    sincosf(ph, &s, &co);
+    const float a1 = hypotf(v.x, v.y), a2 = hypotf(v.z, v.w);
+    v = make_float4(a1 * co, a1 * s, a2 * co, a2 * s);
+    return true;
+}
+
+// normalize_psi (parallel.jl:162-165)
+__device__ __forceinline__ float4 normalize4(float4 v) {
+    const float nrm = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
+    return make_float4(__fdiv_rn(v.x, nrm), __fdiv_rn(v.y, nrm), __fdiv_rn(v.z, nrm), __fdiv_rn(v.w, nrm));
+}
+
+// gauge_transform (parallel.jl:125-129) with real q: psi * exp(-i q)
+__device__ __forceinline__ float4 gauge4(float4 v, float q) {
+    float s, c;
+    sincosf(q, &s, &c);
+    // (a + ib)(c - is) = (ac + bs) + i(bc - as)
+    return make_float4(v.x * c + v.y * s, v.y * c - v.x * s, v.z * c + v.w * s, v.w * c - v.z * s);
+}
+
+}  // namespace isf

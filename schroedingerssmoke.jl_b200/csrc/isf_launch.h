@@ -1,0 +1,42 @@
+// Host-side launchers of the ISF kernels (internal to libisf).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "isf_common.cuh"
+
+namespace isf {
+
+struct XArgs;
+struct YZArgs;
+
+bool supported_len(int n);
+
+cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s);
+cudaError_t launch_yzpass_psi(int op, const YZArgs& a, cudaStream_t s);
+cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s);
+
+// pointwise / stencil kernels (k_point.cu)
+cudaError_t launch_normalize(const Grid& g, float4* psi, cudaStream_t s);
+cudaError_t launch_restrict(const Grid& g, float4* psi, const JetArgs& j, cudaStream_t s);
+cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float len, float rad, cudaStream_t s);
+cudaError_t launch_one_form(const Grid& g, const float4* psi, float* vel, float hbar, int sharp, cudaStream_t s);
+cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s);
+cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s);
+cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s);
+cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s);
+cudaError_t launch_scale_c(const Grid& g, float2* a, float s, cudaStream_t st);
+
+// particles (k_particles.cu)
+struct EmitArgs {
+    float cen[3];
+    float len, rad;
+    uint64_t seed, counter;
+    int mode;
+};
+cudaError_t launch_emit(float* parts, long long nslots, long long start, long long count, const EmitArgs& e,
+                        cudaStream_t s);
+cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel,
+                          unsigned long long* counters, cudaStream_t s);
+
+}  // namespace isf

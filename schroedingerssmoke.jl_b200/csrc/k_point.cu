@@ -1,0 +1,166 @@
+// Pointwise and nearest-neighbour kernels of the ISF API that are not fused
+// into an FFT pass: the standalone forms of normalize_psi, restrict_velocity!,
+// isjet, velocity_one_form! (+ staggered sharp) and div!, and layout
+// conversions of the handle's velocity planes.
+#include "isf_launch.h"
+
+namespace isf {
+
+static inline unsigned grid_for(long long n, int block) {
+    long long b = (n + block - 1) / block;
+    const long long cap = 148LL * 32;  // grid-stride beyond 32 CTAs per SM
+    return (unsigned)(b < cap ? b : cap);
+}
+
+// normalize_psi broadcast (parallel.jl:162-165, examples/benchmark.jl:50)
+__global__ void k_normalize(float4* __restrict__ psi, long long N) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x)
+        psi[c] = normalize4(psi[c]);
+}
+
+// restrict_velocity! (particles.jl:25-27 -> restrict_kernel :12-20)
+__global__ void k_restrict(Grid g, float4* __restrict__ psi, JetArgs j) {
+    const long long N = g.N;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % g.n[0]);
+        const long long r = c / g.n[0];
+        const int y = (int)(r % g.n[1]), z = (int)(r / g.n[1]);
+        float4 v = psi[c];
+        if (restrict_cell(g, j, x, y, z, c, v)) psi[c] = v;
+    }
+}
+
+// isjet.(isf.positions, ...) (particles.jl:6-10, examples/benchmark.jl:26)
+__global__ void k_isjet(Grid g, uint8_t* __restrict__ out, float c0, float c1, float c2, float len, float rad) {
+    const float cen[3] = {c0, c1, c2};
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % g.n[0]);
+        const long long r = c / g.n[0];
+        const int y = (int)(r % g.n[1]), z = (int)(r / g.n[1]);
+        const float px = __fmul_rn((float)x, g.d[0]), py = __fmul_rn((float)y, g.d[1]), pz = __fmul_rn((float)z, g.d[2]);
+        out[c] = isjet_f32(px, py, pz, cen, len, rad) ? 1 : 0;
+    }
+}
+
+// velocity_one_form! (parallel.jl:100-122); with sharp != 0 also the
+// staggered sharp velocity .*= 1 ./ d (examples/benchmark.jl:61-63).
+// Output: three planes vx, vy, vz.
+__global__ void k_one_form(Grid g, const float4* __restrict__ psi, float* __restrict__ vel, float hbar, int sharp) {
+    const long long N = g.N;
+    float* vx = vel;
+    float* vy = vel + N;
+    float* vz = vel + 2 * N;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx);
+        const long long r = c / nx;
+        const int y = (int)(r % ny), z = (int)(r / ny);
+        const long long cxp = (x + 1 == nx) ? c - x : c + 1;
+        const long long cyp = (y + 1 == ny) ? c - (long long)y * nx : c + nx;
+        const long long czp = (z + 1 == nz) ? c - (long long)z * nx * ny : c + (long long)nx * ny;
+        const float4 p = __ldg(&psi[c]);
+        float ax = pair_angle(p, __ldg(&psi[cxp])) * hbar;
+        float ay = pair_angle(p, __ldg(&psi[cyp])) * hbar;
+        float az = pair_angle(p, __ldg(&psi[czp])) * hbar;
+        if (sharp) {
+            ax = __fmul_rn(ax, g.dinv[0]);
+            ay = __fmul_rn(ay, g.dinv[1]);
+            az = __fmul_rn(az, g.dinv[2]);
+        }
+        vx[c] = ax;
+        vy[c] = ay;
+        vz[c] = az;
+    }
+}
+
+// staggered sharp on the handle's velocity (examples/benchmark.jl:61-63)
+__global__ void k_sharp(Grid g, float* __restrict__ vel) {
+    const long long N = g.N;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < 3 * N; c += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(c / N);
+        vel[c] = __fmul_rn(vel[c], g.dinv[a]);
+    }
+}
+
+// div! (parallel.jl:131-152) from the velocity planes
+__global__ void k_div(Grid g, const float* __restrict__ vel, float* __restrict__ f) {
+    const long long N = g.N;
+    const float* vx = vel;
+    const float* vy = vel + N;
+    const float* vz = vel + 2 * N;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(c % nx);
+        const long long r = c / nx;
+        const int y = (int)(r % ny), z = (int)(r / ny);
+        const long long cxm = (x == 0) ? c + nx - 1 : c - 1;
+        const long long cym = (y == 0) ? c + (long long)(ny - 1) * nx : c - nx;
+        const long long czm = (z == 0) ? c + (long long)(nz - 1) * nx * ny : c - (long long)nx * ny;
+        const float t0 = (vx[c] - vx[cxm]) * g.inv_d2[0];
+        const float t1 = (vy[c] - vy[cym]) * g.inv_d2[1];
+        const float t2 = (vz[c] - vz[czm]) * g.inv_d2[2];
+        f[c] = (t0 + t1) + t2;
+    }
+}
+
+__global__ void k_vel_to_aos(Grid g, const float* __restrict__ vel, float* __restrict__ aos) {
+    const long long N = g.N;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        aos[3 * c + 0] = vel[c];
+        aos[3 * c + 1] = vel[N + c];
+        aos[3 * c + 2] = vel[2 * N + c];
+    }
+}
+
+__global__ void k_vel_from_aos(Grid g, const float* __restrict__ aos, float* __restrict__ vel) {
+    const long long N = g.N;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        vel[c] = aos[3 * c + 0];
+        vel[N + c] = aos[3 * c + 1];
+        vel[2 * N + c] = aos[3 * c + 2];
+    }
+}
+
+__global__ void k_scale_c(float2* __restrict__ a, long long N, float s) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x)
+        a[c] = cscale(a[c], s);
+}
+
+cudaError_t launch_scale_c(const Grid& g, float2* a, float s, cudaStream_t st) {
+    k_scale_c<<<grid_for(g.N, 256), 256, 0, st>>>(a, g.N, s);
+    return cudaGetLastError();
+}
+cudaError_t launch_normalize(const Grid& g, float4* psi, cudaStream_t s) {
+    k_normalize<<<grid_for(g.N, 256), 256, 0, s>>>(psi, g.N);
+    return cudaGetLastError();
+}
+cudaError_t launch_restrict(const Grid& g, float4* psi, const JetArgs& j, cudaStream_t s) {
+    k_restrict<<<grid_for(g.N, 256), 256, 0, s>>>(g, psi, j);
+    return cudaGetLastError();
+}
+cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float len, float rad, cudaStream_t s) {
+    k_isjet<<<grid_for(g.N, 256), 256, 0, s>>>(g, out, cen[0], cen[1], cen[2], len, rad);
+    return cudaGetLastError();
+}
+cudaError_t launch_one_form(const Grid& g, const float4* psi, float* vel, float hbar, int sharp, cudaStream_t s) {
+    k_one_form<<<grid_for(g.N, 256), 256, 0, s>>>(g, psi, vel, hbar, sharp);
+    return cudaGetLastError();
+}
+cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s) {
+    k_sharp<<<grid_for(3 * g.N, 256), 256, 0, s>>>(g, vel);
+    return cudaGetLastError();
+}
+cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s) {
+    k_div<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, f);
+    return cudaGetLastError();
+}
+cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s) {
+    k_vel_to_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, aos);
+    return cudaGetLastError();
+}
+cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s) {
+    k_vel_from_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, aos, vel);
+    return cudaGetLastError();
+}
+
+}  // namespace isf

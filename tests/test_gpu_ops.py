@@ -1,0 +1,231 @@
+"""GPU parity of each ISF operator (libisf through the C ABI) against the FP64
+oracle on seeded inputs.  Tolerances: relative L2 error 1e-5 for single
+operators (FP32 arithmetic vs FP64), bit-exact for the integer isjet mask."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import rel, smooth_field, smooth_psi
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [
+    ((4, 2, 2), (16, 8, 8)),
+    ((4, 2, 2), (64, 32, 32)),
+    ((3, 2, 2), (48, 32, 32)),
+    ((6, 3, 3), (96, 48, 48)),
+    ((2, 1, 1), (32, 12, 24)),
+]
+HBAR = float(np.float32(0.1))
+DT = float(np.float32(1 / 48))
+
+
+def cuda(a, dtype=torch.float32):
+    return torch.tensor(np.ascontiguousarray(a), dtype=dtype, device="cuda")
+
+
+def host(t):
+    return t.detach().double().cpu().numpy()
+
+
+@pytest.mark.parametrize("dims", [(16, 8, 8), (32, 12, 24), (48, 32, 32), (96, 48, 48), (256, 128, 128),
+                                  (512, 16, 8), (384, 8, 16), (192, 64, 8)])
+def test_fft3_matches_numpy(isfpkg, dims):
+    isf = isfpkg.ISF((1, 1, 1), dims, HBAR, DT)
+    rng = np.random.default_rng(1)
+    nx, ny, nz = dims
+    a = rng.normal(size=(nz, ny, nx)) + 1j * rng.normal(size=(nz, ny, nx))
+    t = torch.tensor(a.astype(np.complex64), device="cuda")
+    isf.fft3(t, -1)
+    isf.sync()
+    ref = np.fft.fftn(a)
+    assert rel(t.cpu().numpy(), ref) < 2e-6
+    isf.fft3(t, +1)
+    isf.sync()
+    assert rel(t.cpu().numpy(), a) < 2e-6
+
+
+@pytest.mark.parametrize("L,dims", GRIDS)
+def test_schroedinger_flow_and_normalize(isfpkg, oracle_mod, L, dims):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    psi64 = smooth_psi(dims, seed=2)
+    psi = cuda(psi64)
+    isfpkg.schroedinger_flow(isf, psi)
+    isf.sync()
+    orc.schroedinger_flow(psi64)
+    assert rel(host(psi), psi64) < 1e-5
+    # perturb the norm, then normalize
+    psi64 *= 1.0 + 0.3 * np.cos(np.arange(psi64.shape[2]))[None, None, :, None]
+    psi = cuda(psi64)
+    isfpkg.normalize_psi(isf, psi)
+    isf.sync()
+    orc.normalize(psi64)
+    assert rel(host(psi), psi64) < 1e-6
+
+
+@pytest.mark.parametrize("L,dims", GRIDS)
+@pytest.mark.parametrize("hbar", [1.0, HBAR])
+def test_velocity_one_form_and_div(isfpkg, oracle_mod, L, dims, hbar):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    psi64 = smooth_psi(dims, seed=3)
+    psi = cuda(psi64)
+    isfpkg.velocity_one_form(isf, psi, hbar)
+    v = isf.velocity
+    vo = orc.velocity_one_form(psi64, hbar)
+    assert np.abs(host(v) - vo).max() < 2e-6 * max(1.0, hbar)
+    f = isf.div()
+    isf.sync()
+    fo = orc.div()
+    assert rel(host(f), fo) < 1e-4  # difference of nearby angles / d^2: cancellation
+    isfpkg.staggered_sharp(isf)
+    orc.staggered_sharp()
+    assert rel(host(isf.velocity), orc.velocity()) < 1e-6
+
+
+@pytest.mark.parametrize("L,dims", GRIDS)
+def test_poisson_solve(isfpkg, oracle_mod, L, dims):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    rng = np.random.default_rng(4)
+    f = smooth_field(dims, rng, modes=6) + 0.1 * rng.normal(size=dims[::-1])
+    f -= f.mean()
+    q = isf.poisson_solve(cuda(f))
+    isf.sync()
+    orc.set_f(f)
+    qo = orc.poisson_solve()
+    assert np.abs(qo.imag).max() < 1e-10
+    assert rel(host(q), qo.real) < 1e-5
+
+
+@pytest.mark.parametrize("L,dims", GRIDS)
+def test_pressure_project(isfpkg, oracle_mod, L, dims):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    psi64 = smooth_psi(dims, seed=5)
+    psi = cuda(psi64)
+    isfpkg.pressure_project(isf, psi)
+    isf.sync()
+    orc.pressure_project(psi64)
+    assert rel(host(psi), psi64) < 1e-5
+
+
+@pytest.mark.parametrize("L,dims", [((4, 2, 2), (64, 32, 32)), ((4, 2, 2), (128, 64, 64)), ((4, 2, 2), (16, 8, 8))])
+def test_isjet_bit_exact(isfpkg, oracle_mod, cfgs, L, dims):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    noz = cfgs.JET_NOZZLE
+    m = isfpkg.isjet(isf, noz["cen"], noz["len"], noz["rad"])
+    isf.sync()
+    mo = orc.isjet(noz["cen"], noz["len"], noz["rad"])
+    assert m.sum().item() > 0
+    assert np.array_equal(m.cpu().numpy(), mo)
+
+
+@pytest.mark.parametrize("phase_mode", [0, 1])
+@pytest.mark.parametrize("use_mask", [False, True])
+def test_restrict_velocity(isfpkg, oracle_mod, cfgs, phase_mode, use_mask):
+    L, dims = (4, 2, 2), (64, 32, 32)
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    noz = cfgs.JET_NOZZLE
+    kvec, omega = cfgs.jet_omega()
+    psi64 = smooth_psi(dims, seed=6)
+    psi = cuda(psi64)
+    mask = isfpkg.isjet(isf, noz["cen"], noz["len"], noz["rad"]) if use_mask else None
+    isfpkg.restrict_velocity(isf, psi, kvec, mask, omega * 0.5, nozzle=(noz["cen"], noz["len"], noz["rad"]),
+                             phase_mode=phase_mode)
+    isf.sync()
+    orc.restrict_velocity(psi64, kvec, omega * 0.5, noz["cen"], noz["len"], noz["rad"], phase_mode=phase_mode)
+    assert rel(host(psi), psi64) < 2e-6
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_add_particles(isfpkg, oracle_mod, cfgs, mode):
+    L, dims = (4, 2, 2), (64, 32, 32)
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    noz = cfgs.JET_NOZZLE
+    P = 5000
+    parts = torch.full((P, 3), -1.0, device="cuda")
+    isfpkg.add_particles(isf, parts, range(4000, 4000 + 3000), noz["cen"], noz["rad"], seed=11, counter=3,
+                         mode=mode, nozzle_len=noz["len"])
+    isf.sync()
+    for prec, tol in ((32, 2e-6), (64, 2e-6)):
+        orc = oracle_mod.Oracle(L, dims, HBAR, DT, prec=prec)
+        po = np.full((P, 3), -1.0, dtype=orc.dtype)
+        orc.add_particles(po, 4000, 3000, noz["cen"], noz["rad"], seed=11, counter=3, mode=mode,
+                          length=noz["len"])
+        assert np.abs(host(parts) - po).max() < tol
+    # wrapped slots
+    assert (host(parts)[:2000] != -1).all() and (host(parts)[2000:4000] == -1).all()
+
+
+@pytest.mark.parametrize("L,dims", [((4, 2, 2), (64, 32, 32)), ((3, 2, 2), (48, 32, 32))])
+def test_staggered_advect(isfpkg, oracle_mod, L, dims):
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    rng = np.random.default_rng(7)
+    vel = np.stack([smooth_field(dims, rng, scale=0.8) + 0.5 for _ in range(3)], axis=-1)
+    P = 20000
+    parts64 = rng.uniform(0, 1, (P, 3)) * np.asarray(L, np.float64)
+    parts64[:100] = -1.0              # dead slots
+    parts64[100:110, 0] = L[0] + 0.5  # outside the box -> killed
+    parts64 = parts64.astype(np.float32).astype(np.float64)
+    isf.velocity = cuda(vel)
+    orc.set_velocity(vel.astype(np.float32).astype(np.float64))
+    parts = cuda(parts64)
+    isfpkg.staggered_advect(parts, isf)
+    isf.sync()
+    po, margin = orc.staggered_advect(parts64.copy(), margin=True)
+    err = np.abs(host(parts) - po).max(axis=1) / min(L)
+    near_face = margin < 1e-4
+    assert (err[~near_face] < 1e-5).all(), err[~near_face].max()
+    assert near_face.mean() < 0.01
+    assert (host(parts)[:110] == -1).all()
+
+
+@pytest.mark.parametrize("L,dims", [((4, 2, 2), (64, 32, 32)), ((6, 3, 3), (96, 48, 48))])
+def test_step_sequences(isfpkg, oracle_mod, cfgs, L, dims):
+    """isf_step (fused) == oracle simloop body for jet and plain steps."""
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    noz = cfgs.JET_NOZZLE
+    kvec, omega = cfgs.jet_omega()
+    psi64 = cfgs.jet_init_psi(dims)
+    for _ in range(3):
+        orc.restrict_velocity(psi64, kvec, 0.0, noz["cen"], noz["len"], noz["rad"], phase_mode=1)
+        orc.pressure_project(psi64)
+    P = 8000
+    parts64 = np.full((P, 3), -1.0)
+    orc.add_particles(parts64, 0, 2000, noz["cen"], noz["rad"], seed=0, counter=0, mode=1)
+    psi = cuda(psi64)
+    parts = cuda(parts64)
+    margin_min = np.full(P, 1e30)
+    for it in range(1, 6):
+        jet = dict(kvec=kvec, omega_t=float(np.float32(omega) * np.float32(it * np.float32(DT))), cen=noz["cen"],
+                   len=noz["len"], rad=noz["rad"], emit_start=(it * 1000) % P, emit_count=1000, seed=0, counter=it,
+                   emit_mode=1, phase_mode=1)
+        isfpkg.step(isf, psi, parts, jet if it % 2 else None)
+        m = np.zeros(P)
+        orc.step(psi64, parts64, jet if it % 2 else None, margin=m)
+        margin_min = np.minimum(margin_min, m)
+    isf.sync()
+    assert rel(host(psi), psi64) < 2e-5
+    err = np.abs(host(parts) - parts64).max(axis=1) / min(L)
+    ok = margin_min > 1e-4
+    assert (err[ok] < 1e-4).all(), err[ok].max()
+
+
+def test_invalid_arguments(isfpkg):
+    with pytest.raises(isfpkg.ISFError):
+        isfpkg.ISF((1, 1, 1), (20, 8, 8), HBAR, DT)  # 20 is not 2^a 3^b
+    with pytest.raises(isfpkg.ISFError):
+        isfpkg.ISF((1, 1, 1), (8, 8, 8), HBAR, DT)   # nx < 16
+    isf = isfpkg.ISF((1, 1, 1), (16, 8, 8), HBAR, DT)
+    bad = torch.zeros((8, 8, 8, 4), device="cuda")
+    with pytest.raises(isfpkg.ISFError):
+        isfpkg.schroedinger_flow(isf, bad)
+    parts = torch.zeros((10, 3), device="cuda")
+    with pytest.raises(isfpkg.ISFError):
+        isfpkg.add_particles(isf, parts, range(0, 11), (0, 0, 0), 0.1)
