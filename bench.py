@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""ISF time-step benchmark on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl isf|reference]
+
+Workload: the leapfrogging vortex-ring configuration, 256x128x128 grid on a
+10x5x5 torus, hbar 0.1, dt 1/24, 4 194 304 particles seeded in thin tori
+around the rings (no nozzle: one pressure projection per step).  A step is one
+simloop body (examples/benchmark.jl:46-65 of the reference without the jet
+lines): Schroedinger flow, normalize, pressure projection, velocity one-form
++ staggered sharp, RK4 advection of every particle slot.
+
+Printed JSON (rank 0): value = steps/s of the whole job (N independent
+replicas for N > 1, "scaling": "weak"), timed with CUDA events on the
+library's stream over exactly K steps after W warm-up steps, max over ranks.
+The working set (psi 64 MiB, Poisson array 32 MiB, velocity 48 MiB, particles
+48 MiB) is larger than the 126 MB L2, so no flush is needed between steps.
+
+--impl reference times the CPU restatement of the reference's path (FP32,
+OpenMP over all host cores) on the same workload: the reference itself is
+Julia 0.6 code that cannot run here.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ISF steps/s (256x128x128, 4M particles) & adjoint/batched vs plain, 1 B200"
+UNIT = "steps/s"
+WORKLOAD = "vortex_rings_256x128x128_4194304_particles"
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes of each launch site, per grid cell (and per particle slot
+# for the advection): every array a kernel must read or write, once.
+SITE_BYTES_PER_CELL = {
+    "schroedinger x fwd": 32, "schroedinger y fwd": 32, "schroedinger z mask": 32, "schroedinger y inv": 32,
+    "schroedinger x inv": 32,                 # psi read + write
+    "projection div + x fwd": 24,             # psi read, F write
+    "projection y fwd": 16, "projection z fac": 16, "projection y inv": 16,   # F read + write
+    "projection x inv + gauge": 40,           # F read, psi read + write
+    "step one_form": 28,                      # psi read, velocity write
+    "step advect": 12,                        # velocity read (+ 24 B per particle slot)
+}
+STEP_BYTES_PER_CELL = 196      # no-jet step: 64 + 36 + 32 + 52 + 12
+STEP_BYTES_PER_PARTICLE = 24   # position read + write
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["isf", "reference"], default="isf")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_table():
+    """dram bytes per launch per site from the committed ncu summary, if any."""
+    out = {}
+    p = os.path.join(ROOT, "profiles", "ncu_traffic_c3.md")
+    if os.path.exists(p):
+        for line in open(p):
+            parts = line.strip().split("|")
+            if len(parts) >= 4 and parts[1].strip().startswith("site:"):
+                try:
+                    out[parts[1].strip()[5:].strip()] = float(parts[2])
+                except ValueError:
+                    pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "50"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.12)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_workload(cfgs):
+    c = cfgs.CONFIGS["C3"]
+    psi0 = cfgs.vortex_rings_psi(c).astype(np.float32)
+    parts = cfgs.torus_particles(c["particles"], c["rings"], c["ring_yz"], c["torus_minor"], c["seed"])
+    parts = parts[cfgs.cell_sort_order(parts, c["L"], c["dims"])].astype(np.float32)
+    return c, np.ascontiguousarray(psi0), np.ascontiguousarray(parts)
+
+
+def cpu_baseline(c, psi0, parts0, budget_s, steps_cap=None):
+    """FP32 restatement of the reference path on the host cores."""
+    import __graft_entry__ as ge
+    oracle = ge.load_oracle()
+    oracle.build()
+    o = oracle.Oracle(c["L"], c["dims"], c["hbar"], c["dt"], prec=32)
+    psi = psi0.copy()
+    parts = parts0.copy()
+    t0 = time.perf_counter()
+    o.step(psi, parts, None)
+    t1 = time.perf_counter() - t0
+    n = max(1, int(budget_s / max(t1, 1e-3)))
+    if steps_cap is not None:
+        n = min(n, steps_cap)
+    t0 = time.perf_counter()
+    for _ in range(n):
+        o.step(psi, parts, None)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{n} step(s) of {WORKLOAD} after 1 untimed step, FP32 C++ restatement of "
+                      f"src/parallel.jl (OpenMP, own FFT; FFTW is absent)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import __graft_entry__ as ge
+    cfgs = importlib.import_module(ge.load_package().__name__ + ".configs")
+    c, psi0, parts0 = setup_workload(cfgs)
+    budget = max(20.0, min(120.0, 0.5 * (args.steps + args.warmup)))
+    cb = cpu_baseline(c, psi0, parts0, budget, steps_cap=args.steps)
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(c["dims"]), "particles": c["particles"],
+                       "parallelism": "host cores (OpenMP)"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as ge
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pkg = ge.load_package()
+    cfgs = importlib.import_module(pkg.__name__ + ".configs")
+    c, psi0, parts0 = setup_workload(cfgs)
+    P = parts0.shape[0]
+    ncells = int(np.prod(c["dims"]))
+
+    isf = pkg.ISF(c["L"], c["dims"], c["hbar"], c["dt"], device=local)
+    s = isf.stream
+    psi = torch.from_numpy(psi0).to(f"cuda:{local}")
+    parts = torch.from_numpy(parts0).to(f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing
+    for _ in range(args.warmup):
+        pkg.step(isf, psi, parts, None)
+    isf.sync()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = isf.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = ev(), ev()
+    e0.record(s)
+    for _ in range(args.steps):
+        pkg.step(isf, psi, parts, None)
+    e1.record(s)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    gpu_launches = isf.launch_count() - launches0
+    ms = max_over_ranks(ms)
+    value = world * args.steps / (ms / 1000.0)
+    ms_per_step = ms / args.steps
+
+    # ---- per-launch-site timing over a second timed region (roofline)
+    isf.profile_start()
+    for _ in range(args.steps):
+        pkg.step(isf, psi, parts, None)
+    sites = isf.profile_stop()
+    total_site_ms = sum(v[0] for v in sites.values())
+    dom = max(sites, key=lambda k: sites[k][0])
+    dom_ms, dom_n = sites[dom]
+    dom_bytes = SITE_BYTES_PER_CELL.get(dom, 0) * ncells + (STEP_BYTES_PER_PARTICLE * P if dom == "step advect" else 0)
+    peak, peak_kind = measured_hbm()
+    achieved = dom_bytes / (dom_ms / dom_n / 1000.0) / 1e9
+    traffic = traffic_table().get(dom)
+    step_bytes = STEP_BYTES_PER_CELL * ncells + STEP_BYTES_PER_PARTICLE * P
+    step_achieved = step_bytes / (ms_per_step / 1000.0) / 1e9
+
+    # ---- end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_psi = torch.from_numpy(psi0).pin_memory()
+        h_parts = torch.from_numpy(parts0).pin_memory()
+        o_psi = torch.empty_like(h_psi).pin_memory()
+        o_parts = torch.empty_like(h_parts).pin_memory()
+        import ctypes as C
+        L = isf.L
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = ev(), ev()
+        f0.record(s)
+        pkg._lib.check(L.isf_memcpy_h2d(isf.h, C.c_void_p(psi.data_ptr()), C.c_void_p(h_psi.data_ptr()),
+                                        h_psi.numel() * 4), isf.h)
+        pkg._lib.check(L.isf_memcpy_h2d(isf.h, C.c_void_p(parts.data_ptr()), C.c_void_p(h_parts.data_ptr()),
+                                        h_parts.numel() * 4), isf.h)
+        live = 0
+        for _ in range(args.steps):
+            pkg.step(isf, psi, parts, None)
+            live = isf.counters(reset=True)["live"]   # per-step 16-byte device->host read (synchronises)
+        pkg._lib.check(L.isf_memcpy_d2h(isf.h, C.c_void_p(o_psi.data_ptr()), C.c_void_p(psi.data_ptr()),
+                                        o_psi.numel() * 4), isf.h)
+        pkg._lib.check(L.isf_memcpy_d2h(isf.h, C.c_void_p(o_parts.data_ptr()), C.c_void_p(parts.data_ptr()),
+                                        o_parts.numel() * 4), isf.h)
+        f1.record(s)
+        f1.synchronize()
+        ems = max_over_ranks(f0.elapsed_time(f1))
+        state = (h_psi.numel() + h_parts.numel()) * 4
+        e2e = {"value": world * args.steps / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": state / args.steps, "d2h_bytes_per_step": 16 + state / args.steps,
+               "what": "isf_memcpy_h2d of psi0 + particles, K x (isf_step + 16-byte counter read), "
+                       "isf_memcpy_d2h of psi + particles", "live_particles_last_step": live}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    cb = None
+    if not args.no_cpu:
+        cb = cpu_baseline(c, psi0, parts0, args.cpu_seconds)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": list(c["dims"]), "torus": list(c["L"]), "hbar": c["hbar"],
+                   "dt": c["dt"], "particles": P, "jet": False,
+                   "l2": "inputs larger than L2: psi 64 MiB + F 32 MiB + velocity 48 MiB + particles 48 MiB",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                     "launch_ms": dom_ms / dom_n, "share_of_step": dom_ms / total_site_ms},
+        "step_roofline": {"algorithmic_bytes_per_step": step_bytes, "achieved": step_achieved, "peak": peak,
+                          "unit": "GB/s", "frac": step_achieved / peak},
+        "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
+        "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -147,6 +147,19 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
  * of the advections since the last reset */
 ISF_API int isf_counters(isf_handle* h, uint64_t out[2], int32_t reset);
 
+/* ---- tracing (no reference counterpart beyond @time, examples/benchmark.jl:70) */
+
+/* Per-launch-site CUDA-event timing: between start and stop every kernel
+ * launch of h is bracketed by an event pair on h's stream; stop synchronises
+ * and accumulates the elapsed time per launch site (e.g. "proj y fwd"). */
+ISF_API int isf_profile_start(isf_handle* h);
+ISF_API int isf_profile_stop(isf_handle* h);
+ISF_API int isf_profile_sites(const isf_handle* h, int32_t* n);
+ISF_API int isf_profile_get(const isf_handle* h, int32_t i, char* name, size_t cap, double* total_ms,
+                            int64_t* launches);
+/* kernels launched by h since isf_create */
+ISF_API int isf_launch_count(const isf_handle* h, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif

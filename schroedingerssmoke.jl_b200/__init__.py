@@ -136,6 +136,29 @@ class ISF:
         check(self.L.isf_counters(self.h, out, int(reset)), self.h)
         return {"clamp_events": int(out[0]), "live": int(out[1])}
 
+    def launch_count(self) -> int:
+        out = C.c_uint64()
+        check(self.L.isf_launch_count(self.h, C.byref(out)), self.h)
+        return int(out.value)
+
+    def profile_start(self):
+        check(self.L.isf_profile_start(self.h), self.h)
+
+    def profile_stop(self) -> dict:
+        """Stop per-launch-site event timing; {site: (total_ms, launches)}."""
+        check(self.L.isf_profile_stop(self.h), self.h)
+        n = C.c_int32()
+        check(self.L.isf_profile_sites(self.h, C.byref(n)), self.h)
+        out = {}
+        buf = C.create_string_buffer(64)
+        for i in range(n.value):
+            ms = C.c_double()
+            cnt = C.c_int64()
+            check(self.L.isf_profile_get(self.h, i, buf, 64, C.byref(ms), C.byref(cnt)), self.h)
+            if cnt.value:
+                out[buf.value.decode()] = (ms.value, cnt.value)
+        return out
+
     def _psi(self, psi):
         if psi.dtype != torch.float32 or tuple(psi.shape) != self.shape + (4,):
             raise ISFError(_lib.ISF_ERR_INVALID, f"psi must be float32 {self.shape + (4,)}")

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/isf.h"
 #include "isf_launch.h"
@@ -18,10 +19,24 @@ struct isf_handle {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     float2* F = nullptr;     // Poisson spectrum / complex work array, N
+    float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
     float* vel = nullptr;    // velocity planes vx | vy | vz, 3N
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
     unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles
+    unsigned long long launches = 0;         // kernels launched by this handle
     std::string err;
+    // optional per-launch-site event timing (isf_profile_*)
+    struct Rec {
+        int site;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<Rec> recs;
+    std::vector<std::string> site_names;
+    std::vector<double> site_ms;
+    std::vector<long long> site_count;
 };
 
 namespace {
@@ -42,6 +57,50 @@ int cuda_fail(isf_handle* h, cudaError_t e, const char* where) {
 #define ISF_CHECK_HANDLE(h)                                                  \
     do {                                                                     \
         if (!(h)) return fail(nullptr, ISF_ERR_INVALID, "null isf handle");  \
+    } while (0)
+
+int prof_site(isf_handle* h, const char* name) {
+    for (size_t i = 0; i < h->site_names.size(); ++i)
+        if (h->site_names[i] == name) return (int)i;
+    h->site_names.push_back(name);
+    h->site_ms.push_back(0.0);
+    h->site_count.push_back(0);
+    return (int)h->site_names.size() - 1;
+}
+
+cudaEvent_t prof_event(isf_handle* h) {
+    if (h->ev_used == h->ev_pool.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        h->ev_pool.push_back(e);
+    }
+    return h->ev_pool[h->ev_used++];
+}
+
+// Records an event pair around one launch when profiling is on.
+int prof_begin(isf_handle* h, const char* site) {
+    if (!h->prof_on) return -1;
+    isf_handle::Rec r;
+    r.site = prof_site(h, site);
+    r.a = prof_event(h);
+    r.b = prof_event(h);
+    if (!r.a || !r.b) return -1;
+    cudaEventRecord(r.a, h->stream);
+    h->recs.push_back(r);
+    return (int)h->recs.size() - 1;
+}
+
+void prof_end(isf_handle* h, int slot) {
+    if (slot >= 0) cudaEventRecord(h->recs[slot].b, h->stream);
+}
+
+#define ISF_LAUNCH(h, expr, site)                                \
+    do {                                                         \
+        const int ps_ = prof_begin(h, site);                     \
+        cudaError_t e_ = (expr);                                 \
+        ++(h)->launches;                                         \
+        prof_end(h, ps_);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, site);    \
     } while (0)
 
 #define ISF_CUDA(h, expr, where)                      \
@@ -117,27 +176,51 @@ YZArgs yzargs(isf_handle* h, void* data, int axis) {
 int run_schroedinger(isf_handle* h, float* psi, bool norm) {
     XArgs xa = xargs(h);
     xa.psi = reinterpret_cast<float4*>(psi);
-    ISF_CUDA(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
-    ISF_CUDA(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
-    ISF_CUDA(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");
-    ISF_CUDA(h, launch_yzpass_psi(YZ_INV, yzargs(h, psi, 1), h->stream), "schroedinger y inv");
-    ISF_CUDA(h, launch_xpass(norm ? X_PSI_INV_NORM : X_PSI_INV, xa, h->stream), "schroedinger x inv");
+    ISF_LAUNCH(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
+    ISF_LAUNCH(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
+    ISF_LAUNCH(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");
+    ISF_LAUNCH(h, launch_yzpass_psi(YZ_INV, yzargs(h, psi, 1), h->stream), "schroedinger y inv");
+    ISF_LAUNCH(h, launch_xpass(norm ? X_PSI_INV_NORM : X_PSI_INV, xa, h->stream), "schroedinger x inv");
     return ISF_OK;
 }
 
-// pressure_project! with the optional nozzle restriction fused in front
+StencilArgs stargs(isf_handle* h, const float* psi, float* out) {
+    StencilArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.g = h->g;
+    a.psi = reinterpret_cast<const float4*>(psi);
+    a.out = out;
+    return a;
+}
+
+// velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the velocity planes
+int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site) {
+    StencilArgs sa = stargs(h, psi, h->vel);
+    sa.hbar = hbar;
+    sa.sharp = sharp;
+    ISF_LAUNCH(h, launch_stencil(ST_VEL, sa, h->stream), site);
+    return ISF_OK;
+}
+
+// pressure_project! with the optional nozzle restriction fused in front:
+// f = div(one-form) -> Poisson solve -> gauge
 int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
+    StencilArgs sa = stargs(h, psi, h->f);
     XArgs xa = xargs(h);
     xa.psi = reinterpret_cast<float4*>(psi);
+    xa.rin = h->f;
     if (jet) {
+        sa.jet = *jet;
+        sa.use_jet = 1;
         xa.jet = *jet;
         xa.use_jet = 1;
     }
-    ISF_CUDA(h, launch_xpass(X_STENCIL_FWD, xa, h->stream), "projection div + x fwd");
-    ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "projection y fwd");
-    ISF_CUDA(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "projection z fac");
-    ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "projection y inv");
-    ISF_CUDA(h, launch_xpass(X_GAUGE_INV, xa, h->stream), "projection x inv + gauge");
+    ISF_LAUNCH(h, launch_stencil(ST_DIV, sa, h->stream), "projection div");
+    ISF_LAUNCH(h, launch_xpass(X_REAL_FWD, xa, h->stream), "projection x fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "projection y fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "projection z fac");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "projection y inv");
+    ISF_LAUNCH(h, launch_xpass(X_GAUGE_INV, xa, h->stream), "projection x inv + gauge");
     return ISF_OK;
 }
 
@@ -190,6 +273,8 @@ int isf_create(const isf_params* p, isf_handle** out) {
         g.d[a] = (float)((double)p->physical_size[a] / (double)p->grid_res[a]);  // parallel.jl:46
         g.inv_d2[a] = 1.0f / (g.d[a] * g.d[a]);                                  // parallel.jl:150
         g.dinv[a] = 1.0f / g.d[a];                                                // benchmark.jl:62
+        int ex = 0;
+        g.d_pow2[a] = (std::frexp(g.d[a], &ex) == 0.5f) ? 1 : 0;
     }
     g.N = (long long)g.n[0] * g.n[1] * g.n[2];
     g.hbar = p->hbar;
@@ -228,6 +313,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
 
     auto cleanup = [&](int code, const std::string& msg) {
         if (h->F) cudaFree(h->F);
+        if (h->f) cudaFree(h->f);
         if (h->vel) cudaFree(h->vel);
         if (h->tables) cudaFree(h->tables);
         if (h->counters) cudaFree(h->counters);
@@ -242,7 +328,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
         if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: stream: ") + cudaGetErrorString(e));
         h->own_stream = true;
     }
-    if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess ||
+    if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess || cudaMalloc(&h->f, sizeof(float) * g.N) != cudaSuccess ||
         cudaMalloc(&h->vel, sizeof(float) * 3 * g.N) != cudaSuccess ||
         cudaMalloc(&h->tables, total) != cudaSuccess ||
         cudaMalloc(&h->counters, 4 * sizeof(unsigned long long)) != cudaSuccess) {
@@ -271,10 +357,12 @@ int isf_destroy(isf_handle* h) {
         DeviceGuard guard(h->device);
         if (h->stream) cudaStreamSynchronize(h->stream);
         cudaFree(h->F);
+        cudaFree(h->f);
         cudaFree(h->vel);
         cudaFree(h->tables);
         cudaFree(h->counters);
         if (h->own_stream) cudaStreamDestroy(h->stream);
+        for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     }
     delete h;
     return ISF_OK;
@@ -348,7 +436,7 @@ int isf_normalize_psi(isf_handle* h, float* psi) {
     ISF_ENTER(h);
     if (!psi) return fail(h, ISF_ERR_INVALID, "isf_normalize_psi: null psi");
     ISF_ALIGNED(h, psi, 16, "psi");
-    ISF_CUDA(h, launch_normalize(h->g, reinterpret_cast<float4*>(psi), h->stream), "normalize");
+    ISF_LAUNCH(h, launch_normalize(h->g, reinterpret_cast<float4*>(psi), h->stream), "normalize");
     return ISF_OK;
 }
 
@@ -363,34 +451,33 @@ int isf_velocity_one_form(isf_handle* h, const float* psi, float hbar) {
     ISF_ENTER(h);
     if (!psi) return fail(h, ISF_ERR_INVALID, "isf_velocity_one_form: null psi");
     ISF_ALIGNED(h, psi, 16, "psi");
-    ISF_CUDA(h, launch_one_form(h->g, reinterpret_cast<const float4*>(psi), h->vel, hbar, 0, h->stream), "one_form");
-    return ISF_OK;
+    return run_one_form(h, psi, hbar, 0, "one_form");
 }
 
 int isf_staggered_sharp(isf_handle* h) {
     ISF_ENTER(h);
-    ISF_CUDA(h, launch_sharp(h->g, h->vel, h->stream), "staggered_sharp");
+    ISF_LAUNCH(h, launch_sharp(h->g, h->vel, h->stream), "staggered_sharp");
     return ISF_OK;
 }
 
 int isf_get_velocity(isf_handle* h, float* aos) {
     ISF_ENTER(h);
     if (!aos) return fail(h, ISF_ERR_INVALID, "isf_get_velocity: null buffer");
-    ISF_CUDA(h, launch_vel_to_aos(h->g, h->vel, aos, h->stream), "get_velocity");
+    ISF_LAUNCH(h, launch_vel_to_aos(h->g, h->vel, aos, h->stream), "get_velocity");
     return ISF_OK;
 }
 
 int isf_set_velocity(isf_handle* h, const float* aos) {
     ISF_ENTER(h);
     if (!aos) return fail(h, ISF_ERR_INVALID, "isf_set_velocity: null buffer");
-    ISF_CUDA(h, launch_vel_from_aos(h->g, aos, h->vel, h->stream), "set_velocity");
+    ISF_LAUNCH(h, launch_vel_from_aos(h->g, aos, h->vel, h->stream), "set_velocity");
     return ISF_OK;
 }
 
 int isf_isjet(isf_handle* h, uint8_t* mask, const float cen[3], float len, float rad) {
     ISF_ENTER(h);
     if (!mask || !cen) return fail(h, ISF_ERR_INVALID, "isf_isjet: null argument");
-    ISF_CUDA(h, launch_isjet(h->g, mask, cen, len, rad, h->stream), "isjet");
+    ISF_LAUNCH(h, launch_isjet(h->g, mask, cen, len, rad, h->stream), "isjet");
     return ISF_OK;
 }
 
@@ -403,7 +490,7 @@ int isf_restrict_velocity(isf_handle* h, float* psi, const float kvec[3], const 
         return fail(h, ISF_ERR_INVALID, "isf_restrict_velocity: bad phase_mode");
     const float zero[3] = {0.f, 0.f, 0.f};
     JetArgs j = make_jet(kvec, mask, cen ? cen : zero, len, rad, omgterm, phase_mode);
-    ISF_CUDA(h, launch_restrict(h->g, reinterpret_cast<float4*>(psi), j, h->stream), "restrict_velocity");
+    ISF_LAUNCH(h, launch_restrict(h->g, reinterpret_cast<float4*>(psi), j, h->stream), "restrict_velocity");
     return ISF_OK;
 }
 
@@ -421,14 +508,14 @@ int isf_add_particles(isf_handle* h, float* parts, int64_t nslots, int64_t start
     e.seed = seed;
     e.counter = counter;
     e.mode = mode;
-    ISF_CUDA(h, launch_emit(parts, nslots, start % nslots, count, e, h->stream), "add_particles");
+    ISF_LAUNCH(h, launch_emit(parts, nslots, start % nslots, count, e, h->stream), "add_particles");
     return ISF_OK;
 }
 
 int isf_staggered_advect(isf_handle* h, float* parts, int64_t np) {
     ISF_ENTER(h);
     if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_staggered_advect: bad particles");
-    ISF_CUDA(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "staggered_advect");
+    ISF_LAUNCH(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "staggered_advect");
     return ISF_OK;
 }
 
@@ -458,7 +545,7 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
             e.seed = a->seed;
             e.counter = a->counter;
             e.mode = a->emit_mode;
-            ISF_CUDA(h, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, h->stream), "step emit");
+            ISF_LAUNCH(h, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, h->stream), "step emit");
         }
         JetArgs j = make_jet(a->kvec, a->jetmask, a->nozzle_cen, a->nozzle_len, a->nozzle_rad, a->omega_t,
                              a->phase_mode);
@@ -466,16 +553,16 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
         if (rc) return rc;
     }
     // velocity_one_form!(isf, psi, isf.hbar) + staggered sharp
-    ISF_CUDA(h, launch_one_form(h->g, reinterpret_cast<const float4*>(psi), h->vel, h->g.hbar, 1, h->stream),
-             "step one_form");
-    if (np > 0) ISF_CUDA(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "step advect");
+    rc = run_one_form(h, psi, h->g.hbar, 1, "step one_form");
+    if (rc) return rc;
+    if (np > 0) ISF_LAUNCH(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "step advect");
     return ISF_OK;
 }
 
 int isf_div(isf_handle* h, float* f) {
     ISF_ENTER(h);
     if (!f) return fail(h, ISF_ERR_INVALID, "isf_div: null output");
-    ISF_CUDA(h, launch_div(h->g, h->vel, f, h->stream), "div");
+    ISF_LAUNCH(h, launch_div(h->g, h->vel, f, h->stream), "div");
     return ISF_OK;
 }
 
@@ -485,11 +572,11 @@ int isf_poisson_solve(isf_handle* h, const float* f, float* q) {
     XArgs xa = xargs(h);
     xa.rin = f;
     xa.rout = q;
-    ISF_CUDA(h, launch_xpass(X_REAL_FWD, xa, h->stream), "poisson x fwd");
-    ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "poisson y fwd");
-    ISF_CUDA(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "poisson z fac");
-    ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "poisson y inv");
-    ISF_CUDA(h, launch_xpass(X_REAL_INV, xa, h->stream), "poisson x inv");
+    ISF_LAUNCH(h, launch_xpass(X_REAL_FWD, xa, h->stream), "poisson x fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "poisson y fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "poisson z fac");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "poisson y inv");
+    ISF_LAUNCH(h, launch_xpass(X_REAL_INV, xa, h->stream), "poisson x inv");
     return ISF_OK;
 }
 
@@ -500,15 +587,66 @@ int isf_fft3(isf_handle* h, float* data, int32_t sign) {
     XArgs xa = xargs(h);
     xa.F = reinterpret_cast<float2*>(data);
     if (sign < 0) {
-        ISF_CUDA(h, launch_xpass(X_C_FWD, xa, h->stream), "fft3 x");
-        ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 1), h->stream), "fft3 y");
-        ISF_CUDA(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 2), h->stream), "fft3 z");
+        ISF_LAUNCH(h, launch_xpass(X_C_FWD, xa, h->stream), "fft3 x");
+        ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 1), h->stream), "fft3 y");
+        ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, data, 2), h->stream), "fft3 z");
     } else {
-        ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 2), h->stream), "ifft3 z");
-        ISF_CUDA(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 1), h->stream), "ifft3 y");
-        ISF_CUDA(h, launch_xpass(X_C_INV, xa, h->stream), "ifft3 x");
-        ISF_CUDA(h, launch_scale_c(h->g, reinterpret_cast<float2*>(data), (float)h->g.invN, h->stream), "ifft3 scale");
+        ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 2), h->stream), "ifft3 z");
+        ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, data, 1), h->stream), "ifft3 y");
+        ISF_LAUNCH(h, launch_xpass(X_C_INV, xa, h->stream), "ifft3 x");
+        ISF_LAUNCH(h, launch_scale_c(h->g, reinterpret_cast<float2*>(data), (float)h->g.invN, h->stream), "ifft3 scale");
     }
+    return ISF_OK;
+}
+
+int isf_profile_start(isf_handle* h) {
+    ISF_ENTER(h);
+    h->prof_on = true;
+    h->ev_used = 0;
+    h->recs.clear();
+    for (size_t i = 0; i < h->site_ms.size(); ++i) {
+        h->site_ms[i] = 0.0;
+        h->site_count[i] = 0;
+    }
+    return ISF_OK;
+}
+
+int isf_profile_stop(isf_handle* h) {
+    ISF_ENTER(h);
+    h->prof_on = false;
+    ISF_CUDA(h, cudaStreamSynchronize(h->stream), "isf_profile_stop: sync");
+    for (const auto& r : h->recs) {
+        float ms = 0.f;
+        ISF_CUDA(h, cudaEventElapsedTime(&ms, r.a, r.b), "isf_profile_stop: elapsed");
+        h->site_ms[r.site] += ms;
+        h->site_count[r.site] += 1;
+    }
+    h->recs.clear();
+    h->ev_used = 0;
+    return ISF_OK;
+}
+
+int isf_profile_sites(const isf_handle* h, int32_t* n) {
+    if (!h || !n) return fail(nullptr, ISF_ERR_INVALID, "isf_profile_sites: null argument");
+    *n = (int32_t)h->site_names.size();
+    return ISF_OK;
+}
+
+int isf_profile_get(const isf_handle* h, int32_t i, char* name, size_t cap, double* total_ms, int64_t* launches) {
+    if (!h || i < 0 || (size_t)i >= h->site_names.size())
+        return fail(nullptr, ISF_ERR_INVALID, "isf_profile_get: bad index");
+    if (name && cap) {
+        std::strncpy(name, h->site_names[i].c_str(), cap - 1);
+        name[cap - 1] = '\0';
+    }
+    if (total_ms) *total_ms = h->site_ms[i];
+    if (launches) *launches = h->site_count[i];
+    return ISF_OK;
+}
+
+int isf_launch_count(const isf_handle* h, uint64_t* out) {
+    if (!h || !out) return fail(nullptr, ISF_ERR_INVALID, "isf_launch_count: null argument");
+    *out = h->launches;
     return ISF_OK;
 }
 

@@ -20,6 +20,7 @@ struct Grid {
     float d[3];        // Float32(L/n)                      parallel.jl:46
     float inv_d2[3];   // inv.(d .^ 2f0)                    parallel.jl:150
     float dinv[3];     // inv.(d)                           benchmark.jl:62
+    int d_pow2[3];     // d is a power of two: p * dinv == p / d exactly
     float hbar, dt;
     const float2* tw[3];    // tw[a][j] = exp(-2 pi i j / n[a]) rounded from double
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))

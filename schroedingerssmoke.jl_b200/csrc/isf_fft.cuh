@@ -1,27 +1,37 @@
-// Shared-memory Stockham FFT engine for batches of pencils.
+// Register-staged Stockham FFT engine for batches of pencils.
 //
-// One CTA holds C pencils of length N in shared memory as a [N][C] tile of
-// elements T (float2: one complex value; float4: the two psi components,
-// transformed together with shared twiddles).  C * sizeof(T) == 128 bytes,
-// so every pencil position j is one 128-byte shared-memory row and every
-// stage access touches whole rows (bank-conflict free).  The pencil index is
-// XOR-swizzled with the low bits of j so that the transposing global loads of
-// the x pass (lanes walking along j) are conflict free as well.
+// A CTA transforms C pencils of length N.  Each pencil is worked by NT
+// threads; in a stage of radix R every thread owns NBT = ceil(N/R / NT)
+// butterflies and keeps their R inputs in registers:
 //
-// Each stage is a radix-R Stockham step between two buffers (ping-pong):
 //   butterfly i in [0, N/R), span p = product of the earlier radices,
 //   k = i mod p,  x_r = in[i + r N/R] * w^(r k),  w = exp(S 2 pi i / (p R)),
 //   y = DFT_R(x),  out[(i - k) R + k + r p] = y_r.
+//
+// The first stage gathers its inputs straight from the caller's source
+// (global memory, with all loads of a thread issued back to back) and the
+// last stage scatters straight to the caller's sink, so only the stage
+// boundaries in between go through shared memory: one [N][C] tile per CTA,
+// in place (a barrier after every gather and after every scatter).  The
+// tile stores element (j, q) of pencil q at j*C + (q ^ swz(j)); the XOR
+// swizzle keeps row-wise (y/z passes: lanes over q) and column-wise (x pass:
+// lanes over j, including the stride-R scatter of the first stage) accesses
+// free of bank conflicts, since C * sizeof(T) is 128 bytes.
+//
 // Forward transforms use S = -1 (unnormalised), inverse S = +1 (the 1/N of
 // the reference's ifft is folded into the spectral multiply by the callers).
 #pragma once
+#include <initializer_list>
+
 #include "isf_common.cuh"
 
 namespace isf {
 
 template <int C>
 __device__ __forceinline__ int sidx(int j, int q) {
-    return j * C + (q ^ (j & (C - 1)));
+    constexpr int LOG = (C == 8) ? 3 : 4;
+    static_assert(C == 8 || C == 16, "tile width");
+    return j * C + (q ^ ((j ^ (j >> LOG)) & (C - 1)));
 }
 
 // --------------------------------------------------------------- radix DFTs
@@ -81,85 +91,133 @@ __device__ __forceinline__ void dft(T* x) {
     else static_assert(R == 2, "unsupported radix");
 }
 
-// --------------------------------------------------------------- one stage
-template <int N, int C, int NT, int R, int P, int S, class T>
-__device__ __forceinline__ void fft_stage(const T* __restrict__ in, T* __restrict__ out,
-                                          const float2* __restrict__ tw, int q, int t) {
-    constexpr int NB = N / R;
-    static_assert(N % (P * R) == 0, "bad radix plan");
-    constexpr int TS = N / (P * R);  // twiddle table stride
-#pragma unroll 1
-    for (int i = t; i < NB; i += NT) {
-        const int k = i % P;
-        T x[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) x[r] = in[sidx<C>(i + r * NB, q)];
-        if constexpr (P > 1) {
-#pragma unroll
-            for (int r = 1; r < R; ++r) {
-                float2 w = __ldg(&tw[r * k * TS]);  // r*k*TS < N
-                if (S > 0) w.y = -w.y;
-                x[r] = cmul(x[r], w);
-            }
-        }
-        dft<R, S>(x);
-        const int base = (i - k) * R + k;
-#pragma unroll
-        for (int r = 0; r < R; ++r) out[sidx<C>(base + r * P, q)] = x[r];
-    }
-}
-
-template <int N, int C, int NT, int S, class T, int P, int R, int... Rest>
-__device__ __forceinline__ T* run_stages(T* a, T* b, const float2* __restrict__ tw, int q, int t) {
-    fft_stage<N, C, NT, R, P, S, T>(a, b, tw, q, t);
-    __syncthreads();
-    if constexpr (sizeof...(Rest) == 0) {
-        return b;
-    } else {
-        return run_stages<N, C, NT, S, T, P * R, Rest...>(b, a, tw, q, t);
-    }
-}
-
-// Radix plans for the supported pencil lengths (2^a 3^b, 8 <= N <= 512).
-template <int N>
-struct Plan;
-#define ISF_PLAN(NN, FIRST, ...)                                                                  \
-    template <>                                                                                   \
-    struct Plan<NN> {                                                                             \
-        static constexpr int first = FIRST;                                                       \
-        template <int C, int NT, int S, class T>                                                  \
-        static __device__ __forceinline__ T* run(T* a, T* b, const float2* __restrict__ tw, int q, \
-                                                 int t) {                                         \
-            return run_stages<NN, C, NT, S, T, 1, __VA_ARGS__>(a, b, tw, q, t);                   \
-        }                                                                                         \
-    };
-ISF_PLAN(8, 8, 8)
-ISF_PLAN(12, 4, 4, 3)
-ISF_PLAN(16, 4, 4, 4)
-ISF_PLAN(24, 8, 8, 3)
-ISF_PLAN(32, 8, 8, 4)
-ISF_PLAN(48, 4, 4, 4, 3)
-ISF_PLAN(64, 8, 8, 8)
-ISF_PLAN(96, 8, 8, 4, 3)
-ISF_PLAN(128, 8, 8, 4, 4)
-ISF_PLAN(192, 8, 8, 8, 3)
-ISF_PLAN(256, 8, 8, 8, 4)
-ISF_PLAN(384, 8, 8, 4, 4, 3)
-ISF_PLAN(512, 8, 8, 8, 8)
-#undef ISF_PLAN
-
-// threads per pencil: the butterfly count of the first stage, capped so that
-// a CTA of C pencils stays within 1024 threads
-template <int N, int C>
-struct Threads {
-    static constexpr int raw = N / Plan<N>::first;
-    static constexpr int NT = (raw * C > 1024) ? 1024 / C : raw;
-    static constexpr int block = NT * C;
+// ------------------------------------------------------------ stage pieces
+template <int N, int NT, int R>
+struct Stage {
+    static constexpr int NB = N / R;
+    static constexpr int NBT = (NB + NT - 1) / NT;
+    static constexpr int E = NBT * R;
 };
 
-template <int N, int C, int S, class T>
-__device__ __forceinline__ T* fft_pencils(T* a, T* b, const float2* __restrict__ tw, int q, int t) {
-    return Plan<N>::template run<C, Threads<N, C>::NT, S, T>(a, b, tw, q, t);
+// x[b*R + r] := input r of butterfly i = t + b*NT, read through src(j)
+template <int N, int NT, int R, class T, class Src>
+__device__ __forceinline__ void gather(T* x, int t, const Src& src) {
+    constexpr int NB = Stage<N, NT, R>::NB, NBT = Stage<N, NT, R>::NBT;
+#pragma unroll
+    for (int b = 0; b < NBT; ++b) {
+        const int i = t + b * NT;
+        if (NB % NT == 0 || i < NB) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) x[b * R + r] = src(i + r * NB);
+        }
+    }
 }
+
+template <int N, int NT, int R, int P, int S, class T>
+__device__ __forceinline__ void butterflies(T* x, int t, const float2* __restrict__ tw) {
+    constexpr int NB = Stage<N, NT, R>::NB, NBT = Stage<N, NT, R>::NBT;
+    static_assert(N % (P * R) == 0, "bad radix plan");
+    constexpr int TS = N / (P * R);  // twiddle table stride
+#pragma unroll
+    for (int b = 0; b < NBT; ++b) {
+        const int i = t + b * NT;
+        if (NB % NT == 0 || i < NB) {
+            if constexpr (P > 1) {
+                const int k = i % P;
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(&tw[r * k * TS]);  // r*k*TS < N
+                    if (S > 0) w.y = -w.y;
+                    x[b * R + r] = cmul(x[b * R + r], w);
+                }
+            }
+            dft<R, S>(x + b * R);
+        }
+    }
+}
+
+// dst(j, v) for every output j = (i - k) R + k + r P of this thread's butterflies
+template <int N, int NT, int R, int P, class T, class Dst>
+__device__ __forceinline__ void scatter(const T* x, int t, const Dst& dst) {
+    constexpr int NB = Stage<N, NT, R>::NB, NBT = Stage<N, NT, R>::NBT;
+#pragma unroll
+    for (int b = 0; b < NBT; ++b) {
+        const int i = t + b * NT;
+        if (NB % NT == 0 || i < NB) {
+            const int k = i % P;
+            const int base = (i - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) dst(base + r * P, x[b * R + r]);
+        }
+    }
+}
+
+template <int A, int... B>
+struct First {
+    static constexpr int value = A;
+};
+
+// Runs stages (P, R), Rest... on x, which holds the inputs of stage (P, R);
+// intermediate results go through the shared tile sm (pencil q), the final
+// outputs to dst.  Ends without a barrier after the final scatter.
+template <int N, int NT, int C, int S, class T, class Dst, int P, int R, int... Rest>
+__device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2* __restrict__ tw, const Dst& dst) {
+    butterflies<N, NT, R, P, S>(x, t, tw);
+    if constexpr (sizeof...(Rest) == 0) {
+        scatter<N, NT, R, P>(x, t, dst);
+    } else {
+        scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
+        __syncthreads();
+        constexpr int R2 = First<Rest...>::value;
+        gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
+        __syncthreads();
+        pipeline<N, NT, C, S, T, Dst, P * R, Rest...>(x, t, q, sm, tw, dst);
+    }
+}
+
+// --------------------------------------------------------------- radix plans
+constexpr int isf_emax(int N, int NT, std::initializer_list<int> rs) {
+    int m = 0;
+    for (int r : rs) {
+        const int nb = N / r;
+        const int e = ((nb + NT - 1) / NT) * r;
+        m = e > m ? e : m;
+    }
+    return m;
+}
+
+// Supported pencil lengths: 2^a 3^b, 8 <= N <= 512.  NT = N / (first radix).
+template <int N>
+struct Plan;
+#define ISF_PLAN(NN, R0, ...)                                                                               \
+    template <>                                                                                             \
+    struct Plan<NN> {                                                                                       \
+        static constexpr int first = R0;                                                                    \
+        static constexpr int NT = NN / R0;                                                                  \
+        static constexpr int EMAX = isf_emax(NN, NN / R0, {R0, __VA_ARGS__});                               \
+        /* SYNC: barrier after the first gather (needed when src reads the tile) */                       \
+        template <int C, int S, bool SYNC, class T, class Src, class Dst>                                   \
+        static __device__ __forceinline__ void run(T* x, int t, int q, T* sm, const float2* __restrict__ tw, \
+                                                   const Src& src, const Dst& dst) {                        \
+            gather<NN, NN / R0, R0>(x, t, src);                                                             \
+            if constexpr (SYNC) __syncthreads();                                                            \
+            pipeline<NN, NN / R0, C, S, T, Dst, 1, R0, ##__VA_ARGS__>(x, t, q, sm, tw, dst);                \
+        }                                                                                                   \
+    };
+
+ISF_PLAN(8, 8)
+ISF_PLAN(12, 4, 3)
+ISF_PLAN(16, 4, 4)
+ISF_PLAN(24, 8, 3)
+ISF_PLAN(32, 8, 4)
+ISF_PLAN(48, 4, 4, 3)
+ISF_PLAN(64, 8, 8)
+ISF_PLAN(96, 8, 4, 3)
+ISF_PLAN(128, 8, 4, 4)
+ISF_PLAN(192, 8, 8, 3)
+ISF_PLAN(256, 8, 8, 4)
+ISF_PLAN(384, 8, 4, 4, 3)
+ISF_PLAN(512, 8, 8, 8)
+#undef ISF_PLAN
 
 }  // namespace isf

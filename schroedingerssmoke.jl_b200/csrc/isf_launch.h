@@ -16,11 +16,23 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_psi(int op, const YZArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s);
 
-// pointwise / stencil kernels (k_point.cu)
+// z-marching stencils of the one-form (k_stencil.cu)
+enum StOp { ST_DIV = 0, ST_VEL = 1 };
+struct StencilArgs {
+    Grid g;
+    const float4* psi;
+    float* out;  // ST_DIV: f[N]; ST_VEL: vx | vy | vz planes
+    JetArgs jet;
+    int use_jet;
+    float hbar;
+    int sharp;
+};
+cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s);
+
+// pointwise kernels (k_point.cu)
 cudaError_t launch_normalize(const Grid& g, float4* psi, cudaStream_t s);
 cudaError_t launch_restrict(const Grid& g, float4* psi, const JetArgs& j, cudaStream_t s);
 cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float len, float rad, cudaStream_t s);
-cudaError_t launch_one_form(const Grid& g, const float4* psi, float* vel, float hbar, int sharp, cudaStream_t s);
 cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s);
 cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s);
 cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s);

@@ -3,11 +3,14 @@
 // A 3D transform is three axis passes over the array in HBM; each pass is in
 // place and moves every element once (read + write).  Fusions:
 //   Schroedinger step  x fwd | y fwd | z fwd * mask/N, z inv | y inv | x inv + normalize
-//   Poisson solve      x fwd of f = div(one-form(psi)) computed from psi on the fly
-//                      | y fwd | z fwd * fac/N, z inv | y inv | x inv + gauge of psi
+//   Poisson solve      x fwd of the real divergence f | y fwd | z fwd * fac/N, z inv
+//                      | y inv | x inv + gauge of psi (+ the nozzle restriction)
 // so the reference's split/merge broadcasts (parallel.jl:179-180, 185), the
-// complex(f) copy (:169) and the mask / fac multiplies (:171, :182-183) never
-// touch HBM on their own, and velocity and f of the projection are never stored.
+// complex(f) copy (:169), the mask / fac multiplies (:171, :182-183) and the
+// gauge broadcast (:159) never touch HBM on their own.
+//
+// x pass: lanes run along the row (coalesced 512-byte row segments); y / z
+// passes: lanes run across C consecutive x columns (128-byte segments).
 #pragma once
 #include <type_traits>
 
@@ -22,7 +25,6 @@ enum XOp {
     X_PSI_INV_NORM = 2,  // psi rows, inverse, then normalize_psi
     X_C_FWD = 3,         // complex work array F, forward
     X_C_INV = 4,         // complex work array F, inverse
-    X_STENCIL_FWD = 5,   // f = div(one-form(psi)) (optionally of the nozzle-restricted psi) -> F, forward
     X_GAUGE_INV = 6,     // F inverse -> q = Re; psi = gauge(psi (restricted), q)
     X_REAL_FWD = 7,      // real input array -> F, forward
     X_REAL_INV = 8,      // F inverse -> real part to a real output array
@@ -43,96 +45,59 @@ struct XTraits {
     static constexpr bool psi_elems = (OP == X_PSI_FWD || OP == X_PSI_INV || OP == X_PSI_INV_NORM);
     using T = typename std::conditional<psi_elems, float4, float2>::type;
     static constexpr int C = 128 / (int)sizeof(T);
-    static constexpr int S =
-        (OP == X_PSI_FWD || OP == X_C_FWD || OP == X_STENCIL_FWD || OP == X_REAL_FWD) ? -1 : +1;
+    static constexpr int S = (OP == X_PSI_FWD || OP == X_C_FWD || OP == X_REAL_FWD) ? -1 : +1;
 };
 
-__device__ __forceinline__ float4 load_psi_restricted(const XArgs& a, int x, int y, int z) {
-    const long long c = cell(a.g, x, y, z);
-    float4 v = __ldg(&a.psi[c]);
-    if (a.use_jet) restrict_cell(a.g, a.jet, x, y, z, c, v);
-    return v;
-}
-
-// div(velocity_one_form(psi, 1)) at cell (x,y,z): parallel.jl:100-152
-__device__ __forceinline__ float stencil_f(const XArgs& a, int x, int y, int z) {
-    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
-    const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
-    const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-    const int zp = (z + 1 == nz) ? 0 : z + 1, zm = (z == 0) ? nz - 1 : z - 1;
-    const float4 c0 = load_psi_restricted(a, x, y, z);
-    const float4 cxp = load_psi_restricted(a, xp, y, z);
-    const float4 cxm = load_psi_restricted(a, xm, y, z);
-    const float4 cyp = load_psi_restricted(a, x, yp, z);
-    const float4 cym = load_psi_restricted(a, x, ym, z);
-    const float4 czp = load_psi_restricted(a, x, y, zp);
-    const float4 czm = load_psi_restricted(a, x, y, zm);
-    const float vx = pair_angle(c0, cxp), vxm = pair_angle(cxm, c0);
-    const float vy = pair_angle(c0, cyp), vym = pair_angle(cym, c0);
-    const float vz = pair_angle(c0, czp), vzm = pair_angle(czm, c0);
-    const float t0 = (vx - vxm) * a.g.inv_d2[0];
-    const float t1 = (vy - vym) * a.g.inv_d2[1];
-    const float t2 = (vz - vzm) * a.g.inv_d2[2];
-    return (t0 + t1) + t2;
-}
+template <int N, int OP>
+struct XShape {
+    static constexpr int C = XTraits<OP>::C;
+    static constexpr int NT = Plan<N>::NT;
+    static constexpr int BLK = C * NT;
+    static constexpr size_t SMEM = (size_t)N * C * sizeof(typename XTraits<OP>::T);
+};
 
 template <int N, int OP>
-__global__ void __launch_bounds__(Threads<N, XTraits<OP>::C>::block) k_xpass(XArgs a) {
+__global__ void __launch_bounds__(XShape<N, OP>::BLK) k_xpass(XArgs a) {
     using Tr = XTraits<OP>;
     using T = typename Tr::T;
     constexpr int C = Tr::C;
-    constexpr int BLK = Threads<N, C>::block;
+    constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* A = reinterpret_cast<T*>(smraw);
-    T* B = A + N * C;
-    const long long row0 = (long long)blockIdx.x * C;
-    const int tid = threadIdx.x;
-    const int ny = a.g.n[1];
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int t = threadIdx.x % NT, q = threadIdx.x / NT;
+    const long long row = (long long)blockIdx.x * C + q;
+    const long long rb = row * N;
+    T x[Plan<N>::EMAX];
 
-#pragma unroll 1
-    for (int e = tid; e < N * C; e += BLK) {
-        const int q = e / N, j = e - q * N;
-        const long long row = row0 + q;
-        const long long c = row * N + j;
-        T v;
+    auto src = [&](int j) -> T {
         if constexpr (Tr::psi_elems) {
-            v = a.psi[c];
-        } else if constexpr (OP == X_C_FWD || OP == X_C_INV || OP == X_GAUGE_INV) {
-            v = a.F[c];
+            return a.psi[rb + j];
         } else if constexpr (OP == X_REAL_FWD) {
-            v = make_float2(a.rin[c], 0.f);
-        } else {  // X_STENCIL_FWD
-            const int y = (int)(row % ny), z = (int)(row / ny);
-            v = make_float2(stencil_f(a, j, y, z), 0.f);
+            return make_float2(__ldg(&a.rin[rb + j]), 0.f);
+        } else {
+            return a.F[rb + j];
         }
-        A[sidx<C>(j, q)] = v;
-    }
-    __syncthreads();
-    T* R = fft_pencils<N, C, Tr::S>(A, B, a.g.tw[0], tid % C, tid / C);
-
-#pragma unroll 1
-    for (int e = tid; e < N * C; e += BLK) {
-        const int q = e / N, j = e - q * N;
-        const long long row = row0 + q;
-        const long long c = row * N + j;
-        T v = R[sidx<C>(j, q)];
+    };
+    auto dst = [&](int j, const T& v) {
         if constexpr (OP == X_PSI_FWD || OP == X_PSI_INV) {
-            a.psi[c] = v;
+            a.psi[rb + j] = v;
         } else if constexpr (OP == X_PSI_INV_NORM) {
-            a.psi[c] = normalize4(v);
-        } else if constexpr (OP == X_C_FWD || OP == X_C_INV || OP == X_STENCIL_FWD || OP == X_REAL_FWD) {
-            a.F[c] = v;
+            a.psi[rb + j] = normalize4(v);
+        } else if constexpr (OP == X_C_FWD || OP == X_C_INV || OP == X_REAL_FWD) {
+            a.F[rb + j] = v;
         } else if constexpr (OP == X_REAL_INV) {
-            a.rout[c] = v.x;
-        } else {  // X_GAUGE_INV
-            float4 p = a.psi[c];
+            a.rout[rb + j] = v.x;
+        } else {
+            static_assert(OP == X_GAUGE_INV, "unhandled x-pass op");
+            float4 p = a.psi[rb + j];
             if (a.use_jet) {
-                const int y = (int)(row % ny), z = (int)(row / ny);
-                restrict_cell(a.g, a.jet, j, y, z, c, p);
+                const int ny = a.g.n[1];
+                restrict_cell(a.g, a.jet, j, (int)(row % ny), (int)(row / ny), rb + j, p);
             }
-            a.psi[c] = gauge4(p, v.x);
+            a.psi[rb + j] = gauge4(p, v.x);
         }
-    }
+    };
+    Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst);
 }
 
 // -------------------------------------------------------------- y / z pass
@@ -149,32 +114,24 @@ struct YZArgs {
     int axis;  // 1 (y) or 2 (z)
 };
 
-// exp(i (th_x + th_y + th_z)) / N in double, rounded to float: the
-// reference's Float32(exp(i lambda dt / 2)) (parallel.jl:58-62) up to the
-// double rounding of the product.
-__device__ __forceinline__ float2 mask_value(const Grid& g, int kx, int ky, int kz) {
-    const double2 a = g.mtab[0][kx], b = g.mtab[1][ky], c = g.mtab[2][kz];
-    const double abx = a.x * b.x - a.y * b.y, aby = a.x * b.y + a.y * b.x;
-    const double mx = abx * c.x - aby * c.y, my = abx * c.y + aby * c.x;
-    return make_float2((float)(mx * g.invN), (float)(my * g.invN));
-}
+template <int N, class T>
+struct YZShape {
+    static constexpr int C = 128 / (int)sizeof(T);
+    static constexpr int NT = Plan<N>::NT;
+    static constexpr int BLK = C * NT;
+    static constexpr size_t SMEM = (size_t)N * C * sizeof(T);
+};
 
-// fac(k) / N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
-// (parallel.jl:53-55, 63)
-__device__ __forceinline__ float fac_value(const Grid& g, int kx, int ky, int kz) {
-    if ((kx | ky | kz) == 0) return 0.f;
-    const double den = g.s2[0][kx] + g.s2[1][ky] + g.s2[2][kz];
-    return (float)(-0.25 / den * g.invN);
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
 template <int N, class T, int OP>
-__global__ void __launch_bounds__(Threads<N, 128 / (int)sizeof(T)>::block) k_yzpass(YZArgs a) {
-    constexpr int C = 128 / (int)sizeof(T);
-    constexpr int BLK = Threads<N, C>::block;
+__global__ void __launch_bounds__(YZShape<N, T>::BLK) k_yzpass(YZArgs a) {
+    constexpr int C = YZShape<N, T>::C;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* A = reinterpret_cast<T*>(smraw);
-    T* B = A + N * C;
-    const int tid = threadIdx.x;
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int q = threadIdx.x % C, t = threadIdx.x / C;
     const int nx = a.g.n[0], ny = a.g.n[1];
     const int x0 = blockIdx.x * C;
     const int o = blockIdx.y;
@@ -186,44 +143,51 @@ __global__ void __launch_bounds__(Threads<N, 128 / (int)sizeof(T)>::block) k_yzp
         stride = (long long)nx * ny;
         base = x0 + (long long)o * nx;
     }
-    T* data = reinterpret_cast<T*>(a.data);
+    T* __restrict__ data = reinterpret_cast<T*>(a.data);
     const float2* tw = a.g.tw[a.axis];
+    T x[Plan<N>::EMAX];
 
-#pragma unroll 1
-    for (int e = tid; e < N * C; e += BLK) {
-        const int j = e / C, q = e - j * C;
-        A[sidx<C>(j, q)] = data[base + j * stride + q];
-    }
-    __syncthreads();
-    T* R;
-    if constexpr (OP == YZ_INV) {
-        R = fft_pencils<N, C, +1>(A, B, tw, tid % C, tid / C);
+    auto gsrc = [&](int j) -> T { return data[base + j * stride + q]; };
+    auto gdst = [&](int j, const T& v) { data[base + j * stride + q] = v; };
+
+    if constexpr (OP == YZ_FWD) {
+        Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, gdst);
+    } else if constexpr (OP == YZ_INV) {
+        Plan<N>::template run<C, +1, false>(x, t, q, sm, tw, gsrc, gdst);
     } else {
-        R = fft_pencils<N, C, -1>(A, B, tw, tid % C, tid / C);
-    }
-    if constexpr (OP == YZ_MASK || OP == YZ_FAC) {
-#pragma unroll 1
-        for (int e = tid; e < N * C; e += BLK) {
-            const int j = e / C, q = e - j * C;
-            const int kx = x0 + q;
-            const int ky = (a.axis == 1) ? j : o;
-            const int kz = (a.axis == 1) ? o : j;
-            T v = R[sidx<C>(j, q)];
-            if constexpr (OP == YZ_MASK) {
-                v = cmul(v, mask_value(a.g, kx, ky, kz));
-            } else {
-                v = cscale(v, fac_value(a.g, kx, ky, kz));
-            }
-            R[sidx<C>(j, q)] = v;
+        // spectral multiply between the forward and the inverse transform of
+        // this pencil; k along the pass axis is the pencil position j
+        const int kx = x0 + q;
+        const int other = a.axis == 1 ? 2 : 1;
+        if constexpr (OP == YZ_MASK) {
+            // exp(i (th_x + th_y + th_z)) / N in double, rounded to float: the
+            // reference's Float32(exp(i lambda dt / 2)) (parallel.jl:58-62) up
+            // to the double rounding of the product
+            const double2 cxo = zmul(a.g.mtab[0][kx], a.g.mtab[other][o]);
+            const double2* __restrict__ mt = a.g.mtab[a.axis];
+            const double invN = a.g.invN;
+            auto mdst = [&](int j, const T& v) {
+                const double2 m = zmul(cxo, mt[j]);
+                sm[sidx<C>(j, q)] = cmul(v, make_float2((float)(m.x * invN), (float)(m.y * invN)));
+            };
+            Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, mdst);
+        } else {
+            static_assert(OP == YZ_FAC, "unhandled y/z op");
+            // fac(k)/N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
+            // (parallel.jl:53-55, 63)
+            const double dxo = a.g.s2[0][kx] + a.g.s2[other][o];
+            const bool zero_line = (kx == 0) && (o == 0);
+            const double* __restrict__ s2 = a.g.s2[a.axis];
+            const double sc = -0.25 * a.g.invN;
+            auto fdst = [&](int j, const T& v) {
+                const float f = (zero_line && j == 0) ? 0.f : (float)(sc / (dxo + s2[j]));
+                sm[sidx<C>(j, q)] = cscale(v, f);
+            };
+            Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, fdst);
         }
         __syncthreads();
-        T* other = (R == A) ? B : A;
-        R = fft_pencils<N, C, +1>(R, other, tw, tid % C, tid / C);
-    }
-#pragma unroll 1
-    for (int e = tid; e < N * C; e += BLK) {
-        const int j = e / C, q = e - j * C;
-        data[base + j * stride + q] = R[sidx<C>(j, q)];
+        auto ssrc = [&](int j) -> T { return sm[sidx<C>(j, q)]; };
+        Plan<N>::template run<C, +1, true>(x, t, q, sm, tw, ssrc, gdst);
     }
 }
 

@@ -52,15 +52,12 @@ static cudaError_t ensure_smem(K kernel, size_t smem, std::atomic<unsigned long 
 
 template <int N, int OP>
 static cudaError_t launch_x_n(const XArgs& a, cudaStream_t s) {
-    using Tr = XTraits<OP>;
-    constexpr int C = Tr::C;
-    constexpr int BLK = Threads<N, C>::block;
-    const size_t smem = 2ull * N * C * sizeof(typename Tr::T);
+    using Sh = XShape<N, OP>;
     static std::atomic<unsigned long long> done{0};
-    cudaError_t e = ensure_smem(k_xpass<N, OP>, smem, done);
+    cudaError_t e = ensure_smem(k_xpass<N, OP>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    k_xpass<N, OP><<<(unsigned)(rows / C), BLK, smem, s>>>(a);
+    k_xpass<N, OP><<<(unsigned)(rows / Sh::C), Sh::BLK, Sh::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -78,7 +75,6 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
         case X_PSI_INV_NORM: return launch_x_op<X_PSI_INV_NORM>(a, s);
         case X_C_FWD: return launch_x_op<X_C_FWD>(a, s);
         case X_C_INV: return launch_x_op<X_C_INV>(a, s);
-        case X_STENCIL_FWD: return launch_x_op<X_STENCIL_FWD>(a, s);
         case X_GAUGE_INV: return launch_x_op<X_GAUGE_INV>(a, s);
         case X_REAL_FWD: return launch_x_op<X_REAL_FWD>(a, s);
         case X_REAL_INV: return launch_x_op<X_REAL_INV>(a, s);
@@ -88,15 +84,13 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
 
 template <int N, class T, int OP>
 static cudaError_t launch_yz_n(const YZArgs& a, cudaStream_t s) {
-    constexpr int C = 128 / (int)sizeof(T);
-    constexpr int BLK = Threads<N, C>::block;
-    const size_t smem = 2ull * N * C * sizeof(T);
+    using Sh = YZShape<N, T>;
     static std::atomic<unsigned long long> done{0};
-    cudaError_t e = ensure_smem(k_yzpass<N, T, OP>, smem, done);
+    cudaError_t e = ensure_smem(k_yzpass<N, T, OP>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const int other = (a.axis == 1) ? a.g.n[2] : a.g.n[1];
-    dim3 grid((unsigned)(a.g.n[0] / C), (unsigned)other);
-    k_yzpass<N, T, OP><<<grid, BLK, smem, s>>>(a);
+    dim3 grid((unsigned)(a.g.n[0] / Sh::C), (unsigned)other);
+    k_yzpass<N, T, OP><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
     return cudaGetLastError();
 }
 

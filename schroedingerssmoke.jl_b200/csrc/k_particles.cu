@@ -83,8 +83,10 @@ __device__ __forceinline__ float3 stag_vel(const Grid& g, const float* __restric
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float p = jl_modf(P[a], g.L[a]);
-        int ii = (int)floorf(__fdiv_rn(p, g.d[a]));
+        // mod(x, L) is x itself inside [0, L): skip the fmod there
+        const float p = (P[a] >= 0.f && P[a] < g.L[a]) ? P[a] : jl_modf(P[a], g.L[a]);
+        const float qd = g.d_pow2[a] ? p * g.dinv[a] : __fdiv_rn(p, g.d[a]);
+        int ii = (int)floorf(qd);
         if (ii >= g.n[a]) {
             ii = g.n[a] - 1;
             ++clamps;

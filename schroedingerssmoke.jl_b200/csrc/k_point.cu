@@ -1,7 +1,7 @@
 // Pointwise and nearest-neighbour kernels of the ISF API that are not fused
-// into an FFT pass: the standalone forms of normalize_psi, restrict_velocity!,
-// isjet, velocity_one_form! (+ staggered sharp) and div!, and layout
-// conversions of the handle's velocity planes.
+// into an FFT pass or a stencil: the standalone forms of normalize_psi,
+// restrict_velocity!, isjet, the staggered sharp and div! (from the velocity
+// planes), and layout conversions of the handle's velocity planes.
 #include "isf_launch.h"
 
 namespace isf {
@@ -39,37 +39,6 @@ __global__ void k_isjet(Grid g, uint8_t* __restrict__ out, float c0, float c1, f
         const int y = (int)(r % g.n[1]), z = (int)(r / g.n[1]);
         const float px = __fmul_rn((float)x, g.d[0]), py = __fmul_rn((float)y, g.d[1]), pz = __fmul_rn((float)z, g.d[2]);
         out[c] = isjet_f32(px, py, pz, cen, len, rad) ? 1 : 0;
-    }
-}
-
-// velocity_one_form! (parallel.jl:100-122); with sharp != 0 also the
-// staggered sharp velocity .*= 1 ./ d (examples/benchmark.jl:61-63).
-// Output: three planes vx, vy, vz.
-__global__ void k_one_form(Grid g, const float4* __restrict__ psi, float* __restrict__ vel, float hbar, int sharp) {
-    const long long N = g.N;
-    float* vx = vel;
-    float* vy = vel + N;
-    float* vz = vel + 2 * N;
-    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(c % nx);
-        const long long r = c / nx;
-        const int y = (int)(r % ny), z = (int)(r / ny);
-        const long long cxp = (x + 1 == nx) ? c - x : c + 1;
-        const long long cyp = (y + 1 == ny) ? c - (long long)y * nx : c + nx;
-        const long long czp = (z + 1 == nz) ? c - (long long)z * nx * ny : c + (long long)nx * ny;
-        const float4 p = __ldg(&psi[c]);
-        float ax = pair_angle(p, __ldg(&psi[cxp])) * hbar;
-        float ay = pair_angle(p, __ldg(&psi[cyp])) * hbar;
-        float az = pair_angle(p, __ldg(&psi[czp])) * hbar;
-        if (sharp) {
-            ax = __fmul_rn(ax, g.dinv[0]);
-            ay = __fmul_rn(ay, g.dinv[1]);
-            az = __fmul_rn(az, g.dinv[2]);
-        }
-        vx[c] = ax;
-        vy[c] = ay;
-        vz[c] = az;
     }
 }
 
@@ -140,10 +109,6 @@ cudaError_t launch_restrict(const Grid& g, float4* psi, const JetArgs& j, cudaSt
 }
 cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float len, float rad, cudaStream_t s) {
     k_isjet<<<grid_for(g.N, 256), 256, 0, s>>>(g, out, cen[0], cen[1], cen[2], len, rad);
-    return cudaGetLastError();
-}
-cudaError_t launch_one_form(const Grid& g, const float4* psi, float* vel, float hbar, int sharp, cudaStream_t s) {
-    k_one_form<<<grid_for(g.N, 256), 256, 0, s>>>(g, psi, vel, hbar, sharp);
     return cudaGetLastError();
 }
 cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s) {

@@ -1,0 +1,164 @@
+// z-marching stencil kernels of the velocity one-form.
+//
+// One CTA owns a 32 x 8 column block of the grid and walks up to ST_SZ
+// consecutive z planes.  The padded 34 x 10 psi tile of the current plane
+// sits in shared memory, the tile of the next plane arrives in registers
+// while the current one is worked on (prefetch), so psi is read from HBM
+// about once and each angle of the one-form is evaluated about once per cell.
+//
+//   ST_DIV  f = div(velocity_one_form(psi, 1))       parallel.jl:100-122, 131-152
+//           with psi optionally restricted in the nozzle on the fly
+//           (restrict_kernel, particles.jl:12-20)
+//   ST_VEL  velocity planes vx | vy | vz = one_form(psi, hbar) [* 1/d]
+//           (parallel.jl:115-122, staggered sharp examples/benchmark.jl:61-63)
+#include "isf_launch.h"
+
+namespace isf {
+
+namespace {
+
+constexpr int BX = 32, BY = 8, SZ = 16;
+constexpr int TW = BX + 2, TH = BY + 2, TILE = TW * TH;  // padded tile
+constexpr int LPT = (TILE + BX * BY - 1) / (BX * BY);    // tile loads per thread
+
+struct TileLoader {
+    const Grid& g;
+    const StencilArgs& a;
+    int x0, y0;
+    // padded tile element e -> psi at (x0 + c - 1, y0 + r - 1, z), wrapped
+    __device__ __forceinline__ float4 load(int e, int z) const {
+        const int r = e / TW, c = e - r * TW;
+        int x = x0 + c - 1, y = y0 + r - 1;
+        const int nx = g.n[0], ny = g.n[1];
+        x = x < 0 ? x + nx : (x >= nx ? x - nx : x);
+        y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
+        const long long cidx = cell(g, x, y, z);
+        float4 v = __ldg(&a.psi[cidx]);
+        if (a.use_jet) restrict_cell(g, a.jet, x, y, z, cidx, v);
+        return v;
+    }
+};
+
+}  // namespace
+
+template <int OP>
+__global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
+    const Grid& g = a.g;
+    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    const int tid = threadIdx.x, tx = tid & (BX - 1), ty = tid / BX;
+    const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * SZ;
+    // partial tiles: the padded tile keeps its halo at column W+1 / row H+1
+    const int W = min(BX, nx - x0), H = min(BY, ny - y0);
+    const int zend = min(z0 + SZ, nz);
+    const bool own = (tx < W) && (ty < H);
+    const int x = x0 + tx, y = y0 + ty;
+
+    __shared__ float4 tile[2][TH][TW];
+    __shared__ float vxs[BY][BX + 1];  // v_x at x0-1+c (c = 0..W)
+    __shared__ float vys[BY + 1][BX];  // v_y at y0-1+r (r = 0..H)
+
+    const TileLoader ld{g, a, x0, y0};
+    // padded column c <-> x0 + c - 1 (wrapped), so column W+1 is the +x halo
+    // even for a partial tile; columns / rows past the halo repeat it and
+    // stay inside the grid
+    auto tile_e = [&](int e, int z) -> float4 {
+        const int r = e / TW, c = e - r * TW;
+        const int cc = (c > W + 1) ? W + 1 : c;  // unused columns: duplicate the halo
+        const int rr = (r > H + 1) ? H + 1 : r;
+        return ld.load(rr * TW + cc, z);
+    };
+
+    float4 pre[LPT];
+    int cur = 0;
+    // prologue: plane z0 into the tile, plane z0+1 into registers
+#pragma unroll
+    for (int k = 0; k < LPT; ++k) {
+        const int e = tid + k * BX * BY;
+        if (e < TILE) tile[0][e / TW][e % TW] = tile_e(e, z0);
+    }
+    const int z1 = (z0 + 1 == nz) ? 0 : z0 + 1;
+#pragma unroll
+    for (int k = 0; k < LPT; ++k) {
+        const int e = tid + k * BX * BY;
+        if (e < TILE) pre[k] = tile_e(e, z1);
+    }
+    float vz_prev = 0.f;
+    if constexpr (OP == ST_DIV) {
+        float4 pm = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (own) {
+            const int zm = (z0 == 0) ? nz - 1 : z0 - 1;
+            const long long cm = cell(g, x, y, zm);
+            pm = __ldg(&a.psi[cm]);
+            if (a.use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm);
+        }
+        __syncthreads();
+        if (own) vz_prev = pair_angle(pm, tile[0][ty + 1][tx + 1]);
+    }
+
+    for (int z = z0; z < zend; ++z) {
+        __syncthreads();  // tile[cur] complete; previous iteration's reads done
+        const int nxt = cur ^ 1;
+#pragma unroll
+        for (int k = 0; k < LPT; ++k) {
+            const int e = tid + k * BX * BY;
+            if (e < TILE) tile[nxt][e / TW][e % TW] = pre[k];
+        }
+        if (z + 1 < zend) {  // prefetch plane z+2
+            const int z2 = (z + 2 >= nz) ? z + 2 - nz : z + 2;
+#pragma unroll
+            for (int k = 0; k < LPT; ++k) {
+                const int e = tid + k * BX * BY;
+                if (e < TILE) pre[k] = tile_e(e, z2);
+            }
+        }
+        const float4 c0 = tile[cur][ty + 1][tx + 1];
+        if constexpr (OP == ST_DIV) {
+            if (own) {
+                vxs[ty][tx + 1] = pair_angle(c0, tile[cur][ty + 1][tx + 2]);
+                if (tx == 0) vxs[ty][0] = pair_angle(tile[cur][ty + 1][0], c0);
+                vys[ty + 1][tx] = pair_angle(c0, tile[cur][ty + 2][tx + 1]);
+                if (ty == 0) vys[0][tx] = pair_angle(tile[cur][0][tx + 1], c0);
+            }
+            __syncthreads();
+            if (own) {
+                const float vz = pair_angle(c0, tile[nxt][ty + 1][tx + 1]);
+                const float t0 = (vxs[ty][tx + 1] - vxs[ty][tx]) * g.inv_d2[0];
+                const float t1 = (vys[ty + 1][tx] - vys[ty][tx]) * g.inv_d2[1];
+                const float t2 = (vz - vz_prev) * g.inv_d2[2];
+                a.out[cell(g, x, y, z)] = (t0 + t1) + t2;
+                vz_prev = vz;
+            }
+        } else {
+            __syncthreads();
+            if (own) {
+                float ax = pair_angle(c0, tile[cur][ty + 1][tx + 2]) * a.hbar;
+                float ay = pair_angle(c0, tile[cur][ty + 2][tx + 1]) * a.hbar;
+                float az = pair_angle(c0, tile[nxt][ty + 1][tx + 1]) * a.hbar;
+                if (a.sharp) {
+                    ax = __fmul_rn(ax, g.dinv[0]);
+                    ay = __fmul_rn(ay, g.dinv[1]);
+                    az = __fmul_rn(az, g.dinv[2]);
+                }
+                const long long c = cell(g, x, y, z);
+                a.out[c] = ax;
+                a.out[g.N + c] = ay;
+                a.out[2 * g.N + c] = az;
+            }
+        }
+        cur = nxt;
+    }
+}
+
+cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
+    dim3 grid((unsigned)((a.g.n[0] + BX - 1) / BX), (unsigned)((a.g.n[1] + BY - 1) / BY),
+              (unsigned)((a.g.n[2] + SZ - 1) / SZ));
+    if (op == ST_DIV)
+        k_stencil<ST_DIV><<<grid, BX * BY, 0, s>>>(a);
+    else if (op == ST_VEL)
+        k_stencil<ST_VEL><<<grid, BX * BY, 0, s>>>(a);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+}  // namespace isf
