@@ -143,9 +143,12 @@ ISF_API int isf_poisson_solve(isf_handle* h, const float* f_dev, float* q_dev);
 /* in-place 3D complex FFT of interleaved complex64 data, sign -1 forward
  * (unnormalised), +1 inverse (1/N): the plan_fft! / plan_ifft! of src/parallel.jl:79 */
 ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
-/* clamp events (staggered_velocity index rounded to n+1) and live particles
- * of the advections since the last reset */
-ISF_API int isf_counters(isf_handle* h, uint64_t out[2], int32_t reset);
+/* First n (<= 16) counters of the advections since the last reset: [0] clamp
+ * events (staggered_velocity index rounded to n+1), [1] live particles; in a
+ * bounds-checking build (-DISF_CHECK) [2] rejected gather indices, [3] the
+ * first of them and [4..11] its cell indices, +1 neighbours and strides.
+ * Synchronises the handle's stream. */
+ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);
 
 /* ---- tracing (no reference counterpart beyond @time, examples/benchmark.jl:70) */
 

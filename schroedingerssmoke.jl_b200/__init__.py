@@ -132,9 +132,11 @@ class ISF:
         return a
 
     def counters(self, reset: bool = False):
-        out = (C.c_uint64 * 2)()
-        check(self.L.isf_counters(self.h, out, int(reset)), self.h)
-        return {"clamp_events": int(out[0]), "live": int(out[1])}
+        """Advection counters since the last reset (see isf_counters)."""
+        out = (C.c_uint64 * 16)()
+        check(self.L.isf_counters(self.h, out, 16, int(reset)), self.h)
+        return {"clamp_events": int(out[0]), "live": int(out[1]), "check_failures": int(out[2]),
+                "first_bad_index": int(out[3]), "first_bad_context": [int(v) for v in out[4:12]]}
 
     def launch_count(self) -> int:
         out = C.c_uint64()

@@ -68,11 +68,12 @@ _lib = None
 
 
 def load(path: str | None = None):
-    """Load libisf.so and declare its signatures."""
+    """Load libisf.so (or the library named by $ISF_LIBRARY, e.g. the
+    bounds-checking libisf_check.so) and declare its signatures."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("ISF_LIBRARY") or LIB_PATH
     if not os.path.exists(p):
         raise ImportError(f"libisf.so not built ({p}); run schroedingerssmoke.jl_b200/build.py")
     L = C.CDLL(p)
@@ -103,7 +104,7 @@ def load(path: str | None = None):
         "isf_div": [vp, vp],
         "isf_poisson_solve": [vp, vp, vp],
         "isf_fft3": [vp, vp, i32],
-        "isf_counters": [vp, C.POINTER(C.c_uint64), i32],
+        "isf_counters": [vp, C.POINTER(C.c_uint64), i32, i32],
         "isf_profile_start": [vp],
         "isf_profile_stop": [vp],
         "isf_profile_sites": [vp, C.POINTER(C.c_int32)],

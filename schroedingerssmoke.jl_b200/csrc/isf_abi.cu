@@ -20,9 +20,9 @@ struct isf_handle {
     bool own_stream = false;
     float2* F = nullptr;     // Poisson spectrum / complex work array, N
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
-    float* vel = nullptr;    // velocity planes vx | vy | vz, 3N
+    float* vel = nullptr;    // velocity, float4 (vx, vy, vz, 0) per cell, 4N
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
-    unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles
+    unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
     unsigned long long launches = 0;         // kernels launched by this handle
     std::string err;
     // optional per-launch-site event timing (isf_profile_*)
@@ -193,7 +193,7 @@ StencilArgs stargs(isf_handle* h, const float* psi, float* out) {
     return a;
 }
 
-// velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the velocity planes
+// velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the handle's velocity
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site) {
     StencilArgs sa = stargs(h, psi, h->vel);
     sa.hbar = hbar;
@@ -329,15 +329,15 @@ int isf_create(const isf_params* p, isf_handle** out) {
         h->own_stream = true;
     }
     if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess || cudaMalloc(&h->f, sizeof(float) * g.N) != cudaSuccess ||
-        cudaMalloc(&h->vel, sizeof(float) * 3 * g.N) != cudaSuccess ||
+        cudaMalloc(&h->vel, sizeof(float4) * g.N) != cudaSuccess ||
         cudaMalloc(&h->tables, total) != cudaSuccess ||
-        cudaMalloc(&h->counters, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaMalloc(&h->counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
         return cleanup(ISF_ERR_NOMEM, "isf_create: device allocation failed");
     }
     e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 4 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float) * 3 * g.N);
+    if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float4) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
     char* base = reinterpret_cast<char*>(h->tables);
     off = 0;
@@ -515,6 +515,7 @@ int isf_add_particles(isf_handle* h, float* parts, int64_t nslots, int64_t start
 int isf_staggered_advect(isf_handle* h, float* parts, int64_t np) {
     ISF_ENTER(h);
     if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_staggered_advect: bad particles");
+    if (np > kMaxParticles) return fail(h, ISF_ERR_INVALID, "isf_staggered_advect: more than 715827882 particles");
     ISF_LAUNCH(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "staggered_advect");
     return ISF_OK;
 }
@@ -524,6 +525,7 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     if (!psi || !a) return fail(h, ISF_ERR_INVALID, "isf_step: null argument");
     ISF_ALIGNED(h, psi, 16, "psi");
     if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_step: bad particles");
+    if (np > kMaxParticles) return fail(h, ISF_ERR_INVALID, "isf_step: more than 715827882 particles");
     if (a->jet) {
         if (a->phase_mode != ISF_PHASE_REFERENCE_SUM && a->phase_mode != ISF_PHASE_DOT)
             return fail(h, ISF_ERR_INVALID, "isf_step: bad phase_mode");
@@ -650,16 +652,14 @@ int isf_launch_count(const isf_handle* h, uint64_t* out) {
     return ISF_OK;
 }
 
-int isf_counters(isf_handle* h, uint64_t out[2], int32_t reset) {
+int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset) {
     ISF_ENTER(h);
-    unsigned long long tmp[2] = {0, 0};
+    if (n < 0 || n > 16 || (n > 0 && !out)) return fail(h, ISF_ERR_INVALID, "isf_counters: n must be 0..16");
+    unsigned long long tmp[16] = {0};
     ISF_CUDA(h, cudaMemcpyAsync(tmp, h->counters, sizeof(tmp), cudaMemcpyDeviceToHost, h->stream), "counters");
     ISF_CUDA(h, cudaStreamSynchronize(h->stream), "counters sync");
-    if (out) {
-        out[0] = tmp[0];
-        out[1] = tmp[1];
-    }
-    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, 2 * sizeof(unsigned long long), h->stream), "counters reset");
+    for (int i = 0; i < n; ++i) out[i] = tmp[i];
+    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, sizeof(tmp), h->stream), "counters reset");
     return ISF_OK;
 }
 

@@ -4,7 +4,7 @@
 //   cell index  c = x + nx*(y + ny*z)  (column-major, x fastest)
 //   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
 //               == NTuple{2,ComplexF32} of src/parallel.jl
-//   velocity    three planes vx[N], vy[N], vz[N] (SoA, internal to the handle)
+//   velocity    float4 (vx, vy, vz, 0) per cell (internal to the handle)
 //   F           float2 per cell: the Poisson spectrum work array
 //   particles   float3 per slot (AoS), dead slot = (-1,-1,-1)
 #pragma once
@@ -58,12 +58,37 @@ __host__ __device__ __forceinline__ long long cell(const Grid& g, int x, int y, 
     return (long long)x + (long long)g.n[0] * ((long long)y + (long long)g.n[1] * z);
 }
 
+// atan2(y, x) for the one-form angles: t = min(|x|,|y|) / max(|x|,|y|) in
+// [0, 1], atan(t) = t P(t^2) with the degree-8 polynomial fitted by
+// csrc/gen_atan_coeffs.py (Remez exchange, max error 1.1e-7 in float32), then
+// the octant / quadrant fix-ups.  |error| <= 2.5e-7 rad for finite inputs;
+// angle(0) = 0 as in Julia.
+__device__ __forceinline__ float isf_atan2(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    const float t = (mx > 0.f) ? __fdividef(mn, mx) : 0.f;
+    const float s = t * t;
+    float p = 2.456725575e-03f;
+    p = fmaf(p, s, -1.440136135e-02f);
+    p = fmaf(p, s, 3.978123143e-02f);
+    p = fmaf(p, s, -7.234857976e-02f);
+    p = fmaf(p, s, 1.049894616e-01f);
+    p = fmaf(p, s, -1.416122913e-01f);
+    p = fmaf(p, s, 1.998590678e-01f);
+    p = fmaf(p, s, -3.333259821e-01f);
+    p = fmaf(p, s, 9.999998808e-01f);
+    float a = t * p;
+    if (ay > ax) a = 1.57079632679489662f - a;
+    if (x < 0.f) a = 3.14159265358979324f - a;
+    return copysignf(a, y);
+}
+
 // Julia `angle(conj(a1)*b1 + conj(a2)*b2)` for psi pairs a, b (parallel.jl:108-111)
 __device__ __forceinline__ float pair_angle(float4 a, float4 b) {
     // conj(a1)*b1 = (a.x - i a.y)(b.x + i b.y)
     float re = a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w;
     float im = a.x * b.y - a.y * b.x + a.z * b.w - a.w * b.z;
-    return atan2f(im, re);
+    return isf_atan2(im, re);
 }
 
 // particles.jl:6-10, evaluated in float with every operation rounded on its

@@ -21,7 +21,7 @@ enum StOp { ST_DIV = 0, ST_VEL = 1 };
 struct StencilArgs {
     Grid g;
     const float4* psi;
-    float* out;  // ST_DIV: f[N]; ST_VEL: vx | vy | vz planes
+    float* out;  // ST_DIV: f[N]; ST_VEL: float4 (vx, vy, vz, 0) per cell
     JetArgs jet;
     int use_jet;
     float hbar;
@@ -39,7 +39,8 @@ cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaS
 cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s);
 cudaError_t launch_scale_c(const Grid& g, float2* a, float s, cudaStream_t st);
 
-// particles (k_particles.cu)
+// particles (k_particles.cu); slot indices are 32-bit: 3 * np < 2^31
+constexpr long long kMaxParticles = 715827882LL;
 struct EmitArgs {
     float cen[3];
     float len, rad;

@@ -64,84 +64,121 @@ __global__ void k_emit(float* __restrict__ parts, long long nslots, long long st
     parts[3 * s + 2] = p2;
 }
 
-// Julia's mod(x, y) for floats (sign of y; r + y rounded)
-__device__ __forceinline__ float jl_modf(float x, float y) {
-    float r = fmodf(x, y);
-    if (r == 0.f) return copysignf(0.f, y);
-    if ((r > 0.f) != (y > 0.f)) r += y;
+// Julia's mod(x, L) for floats and L > 0 (rem, then + L when negative, the
+// addition rounded).  RK sample points lie within one box length of [0, L)
+// in practice, where the result needs no fmod: for x in [L, 2L), fmod(x, L) =
+// x - L is exact (Sterbenz); for x in (-L, 0), fmod(x, L) = x and the
+// reference adds L.  Other values take the general path.
+__device__ __forceinline__ float jl_mod_box(float x, float L) {
+    if (x >= 0.f && x < L) return x;
+    if (x >= L && x < 2.f * L) return x - L;
+    if (x < 0.f && x > -L) return x + L;
+    float r = fmodf(x, L);
+    if (r == 0.f) return 0.f;  // copysign(0, L)
+    if (r < 0.f) r += L;
     return r;
 }
 
-// staggered_velocity (parallel.jl:219-246).  Interpolation weights are the
+// staggered_velocity (parallel.jl:219-246) on the handle's velocity
+// (float4 (vx, vy, vz, 0) per cell).  Interpolation weights are the
 // reference's unnormalised w = p - (i-1) d.  An index that rounds to n (p
 // rounded up to L by mod) is clamped to the last cell and counted.
-__device__ __forceinline__ float3 stag_vel(const Grid& g, const float* __restrict__ vx,
-                                           const float* __restrict__ vy, const float* __restrict__ vz, float3 pt,
-                                           unsigned& clamps) {
+// POW2: every d is a power of two, so p * (1/d) == p / d exactly.
+// Gather of one velocity cell.  With -DISF_CHECK (debug builds) every index
+// is validated; a bad one is recorded in chk[0..1] (count, first index) and
+// replaced by cell 0 instead of being read.
+__device__ __forceinline__ float4 vload(const Grid& g, const float4* __restrict__ v, int c,
+                                        unsigned long long* chk, const int* ctx) {
+#ifdef ISF_CHECK
+    if (c < 0 || (long long)c >= g.N) {
+        if (chk) {
+            if (atomicAdd(&chk[0], 1ull) == 0) {
+                chk[1] = (unsigned long long)(unsigned)c;
+                for (int k = 0; k < 8; ++k) chk[2 + k] = (unsigned long long)(unsigned)ctx[k];
+            }
+        }
+        c = 0;
+    }
+#else
+    (void)g;
+    (void)chk;
+    (void)ctx;
+#endif
+    return __ldg(&v[c]);
+}
+
+template <bool POW2>
+__device__ __forceinline__ float3 stag_vel(const Grid& g, const float4* __restrict__ v, float3 pt,
+                                           unsigned& clamps, unsigned long long* chk) {
     const float P[3] = {pt.x, pt.y, pt.z};
     int i[3], ip[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        // mod(x, L) is x itself inside [0, L): skip the fmod there
-        const float p = (P[a] >= 0.f && P[a] < g.L[a]) ? P[a] : jl_modf(P[a], g.L[a]);
-        const float qd = g.d_pow2[a] ? p * g.dinv[a] : __fdiv_rn(p, g.d[a]);
-        int ii = (int)floorf(qd);
-        if (ii >= g.n[a]) {
-            ii = g.n[a] - 1;
+        const float p = jl_mod_box(P[a], g.L[a]);
+        const float qd = POW2 ? p * g.dinv[a] : __fdiv_rn(p, g.d[a]);
+        const int nm = g.n[a] - 1;
+        int ii = __float2int_rd(qd);  // UInt32(floor(p / d))
+        if (ii > nm) {
+            ii = nm;
             ++clamps;
         }
         if (ii < 0) ii = 0;
         i[a] = ii;
-        ip[a] = (ii + 1 == g.n[a]) ? 0 : ii + 1;
+        ip[a] = (ii < nm) ? ii + 1 : 0;  // mod(i, res) + 1 (periodic +1 neighbour)
         w[a] = __fsub_rn(p, __fmul_rn((float)ii, g.d[a]));
     }
-    const long long nx = g.n[0], nxy = (long long)g.n[0] * g.n[1];
-    const long long i0 = i[0], j0 = (long long)i[1] * nx, k0 = (long long)i[2] * nxy;
-    const long long i1 = ip[0], j1 = (long long)ip[1] * nx, k1 = (long long)ip[2] * nxy;
-    // u_x: bilinear in (y, z) over x-edge samples
-    const float x00 = __ldg(&vx[i0 + j0 + k0]), x10 = __ldg(&vx[i0 + j1 + k0]);
-    const float x01 = __ldg(&vx[i0 + j0 + k1]), x11 = __ldg(&vx[i0 + j1 + k1]);
-    // u_y: bilinear in (x, z)
-    const float y00 = __ldg(&vy[i0 + j0 + k0]), y10 = __ldg(&vy[i1 + j0 + k0]);
-    const float y01 = __ldg(&vy[i0 + j0 + k1]), y11 = __ldg(&vy[i1 + j0 + k1]);
-    // u_z: bilinear in (x, y)
-    const float z00 = __ldg(&vz[i0 + j0 + k0]), z10 = __ldg(&vz[i1 + j0 + k0]);
-    const float z01 = __ldg(&vz[i0 + j1 + k0]), z11 = __ldg(&vz[i1 + j1 + k0]);
+    const int nx = g.n[0], nxy = g.n[0] * g.n[1];
+    const int ry0 = i[1] * nx, ry1 = ip[1] * nx, rz0 = i[2] * nxy, rz1 = ip[2] * nxy;
+    const int c000 = i[0] + ry0 + rz0;
+    const int c100 = ip[0] + ry0 + rz0, c010 = i[0] + ry1 + rz0, c001 = i[0] + ry0 + rz1;
+    const int c011 = i[0] + ry1 + rz1, c101 = ip[0] + ry0 + rz1, c110 = ip[0] + ry1 + rz0;
+#ifdef ISF_CHECK
+    const int ctx[8] = {i[0], i[1], i[2], ip[0], ip[1], ip[2], nx, nxy};
+#else
+    const int* ctx = nullptr;
+#endif
+    const float4 v000 = vload(g, v, c000, chk, ctx);
+    const float4 v100 = vload(g, v, c100, chk, ctx);    // pxp
+    const float4 v010 = vload(g, v, c010, chk, ctx);    // pyp
+    const float4 v001 = vload(g, v, c001, chk, ctx);    // pzp
+    const float x11 = vload(g, v, c011, chk, ctx).x;    // velocity[i, jp, kp][1]
+    const float y11 = vload(g, v, c101, chk, ctx).y;    // velocity[ip, j, kp][2]
+    const float z11 = vload(g, v, c110, chk, ctx).z;    // velocity[ip, jp, k][3]
+    const float wx = w[0], wy = w[1], wz = w[2];
     float3 u;
-    u.x = (1.f - w[2]) * ((1.f - w[1]) * x00 + w[1] * x10) + w[2] * ((1.f - w[1]) * x01 + w[1] * x11);
-    u.y = (1.f - w[2]) * ((1.f - w[0]) * y00 + w[0] * y10) + w[2] * ((1.f - w[0]) * y01 + w[0] * y11);
-    u.z = (1.f - w[1]) * ((1.f - w[0]) * z00 + w[0] * z10) + w[1] * ((1.f - w[0]) * z01 + w[0] * z11);
+    u.x = (1.f - wz) * ((1.f - wy) * v000.x + wy * v010.x) + wz * ((1.f - wy) * v001.x + wy * x11);
+    u.y = (1.f - wz) * ((1.f - wx) * v000.y + wx * v100.y) + wz * ((1.f - wx) * v001.y + wx * y11);
+    u.z = (1.f - wy) * ((1.f - wx) * v000.z + wx * v100.z) + wy * ((1.f - wx) * v010.z + wx * z11);
     return u;
 }
 
 // staggered_advect! (parallel.jl:197-216, 248-261): classical RK4 for every
 // slot inside the open box 0 < p < L, (-1,-1,-1) otherwise.
 // counters[0] accumulates clamp events, counters[1] live particles.
-__global__ void k_advect(Grid g, float* __restrict__ parts, long long np, const float* __restrict__ vel,
-                         unsigned long long* __restrict__ counters) {
-    const long long N = g.N;
-    const float* vx = vel;
-    const float* vy = vel + N;
-    const float* vz = vel + 2 * N;
+template <bool POW2>
+__global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
+                                                const float4* __restrict__ vel,
+                                                unsigned long long* __restrict__ counters) {
     unsigned clamps = 0, live = 0;
-    const float dt = g.dt;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < np; k += (long long)gridDim.x * blockDim.x) {
+    unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
+    const float dt = g.dt, s6 = g.dt / 6.0f;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
         float3 p = make_float3(parts[3 * k], parts[3 * k + 1], parts[3 * k + 2]);
         const bool inside = (p.x > 0.f && p.x < g.L[0]) && (p.y > 0.f && p.y < g.L[1]) && (p.z > 0.f && p.z < g.L[2]);
         if (inside) {
             ++live;
-            const float3 k1 = stag_vel(g, vx, vy, vz, p, clamps);
+            // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
+            const float3 k1 = stag_vel<POW2>(g, vel, p, clamps, chk);
             float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-            const float3 k2 = stag_vel(g, vx, vy, vz, q, clamps);
+            const float3 k2 = stag_vel<POW2>(g, vel, q, clamps, chk);
             q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-            const float3 k3 = stag_vel(g, vx, vy, vz, q, clamps);
+            const float3 k3 = stag_vel<POW2>(g, vel, q, clamps, chk);
             q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-            const float3 k4 = stag_vel(g, vx, vy, vz, q, clamps);
-            const float s = dt / 6.0f;
-            p.x = p.x + s * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
-            p.y = p.y + s * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
-            p.z = p.z + s * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
+            const float3 k4 = stag_vel<POW2>(g, vel, q, clamps, chk);
+            p.x = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
+            p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
+            p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
         } else {
             p = make_float3(-1.f, -1.f, -1.f);
         }
@@ -174,10 +211,15 @@ cudaError_t launch_emit(float* parts, long long nslots, long long start, long lo
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel, unsigned long long* counters,
                           cudaStream_t s) {
     if (np <= 0) return cudaSuccess;
+    if (np > kMaxParticles) return cudaErrorInvalidValue;
     const int blk = 256;
     long long b = (np + blk - 1) / blk;
     if (b > 148LL * 64) b = 148LL * 64;
-    k_advect<<<(unsigned)b, blk, 0, s>>>(g, parts, np, vel, counters);
+    const float4* v = reinterpret_cast<const float4*>(vel);
+    if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
+        k_advect<true><<<(unsigned)b, blk, 0, s>>>(g, parts, (int)np, v, counters);
+    else
+        k_advect<false><<<(unsigned)b, blk, 0, s>>>(g, parts, (int)np, v, counters);
     return cudaGetLastError();
 }
 

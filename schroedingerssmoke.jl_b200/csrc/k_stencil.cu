@@ -9,7 +9,7 @@
 //   ST_DIV  f = div(velocity_one_form(psi, 1))       parallel.jl:100-122, 131-152
 //           with psi optionally restricted in the nozzle on the fly
 //           (restrict_kernel, particles.jl:12-20)
-//   ST_VEL  velocity planes vx | vy | vz = one_form(psi, hbar) [* 1/d]
+//   ST_VEL  velocity (vx, vy, vz, 0) per cell = one_form(psi, hbar) [* 1/d]
 //           (parallel.jl:115-122, staggered sharp examples/benchmark.jl:61-63)
 #include "isf_launch.h"
 
@@ -20,24 +20,6 @@ namespace {
 constexpr int BX = 32, BY = 8, SZ = 16;
 constexpr int TW = BX + 2, TH = BY + 2, TILE = TW * TH;  // padded tile
 constexpr int LPT = (TILE + BX * BY - 1) / (BX * BY);    // tile loads per thread
-
-struct TileLoader {
-    const Grid& g;
-    const StencilArgs& a;
-    int x0, y0;
-    // padded tile element e -> psi at (x0 + c - 1, y0 + r - 1, z), wrapped
-    __device__ __forceinline__ float4 load(int e, int z) const {
-        const int r = e / TW, c = e - r * TW;
-        int x = x0 + c - 1, y = y0 + r - 1;
-        const int nx = g.n[0], ny = g.n[1];
-        x = x < 0 ? x + nx : (x >= nx ? x - nx : x);
-        y = y < 0 ? y + ny : (y >= ny ? y - ny : y);
-        const long long cidx = cell(g, x, y, z);
-        float4 v = __ldg(&a.psi[cidx]);
-        if (a.use_jet) restrict_cell(g, a.jet, x, y, z, cidx, v);
-        return v;
-    }
-};
 
 }  // namespace
 
@@ -57,31 +39,44 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
     __shared__ float vxs[BY][BX + 1];  // v_x at x0-1+c (c = 0..W)
     __shared__ float vys[BY + 1][BX];  // v_y at y0-1+r (r = 0..H)
 
-    const TileLoader ld{g, a, x0, y0};
-    // padded column c <-> x0 + c - 1 (wrapped), so column W+1 is the +x halo
-    // even for a partial tile; columns / rows past the halo repeat it and
-    // stay inside the grid
-    auto tile_e = [&](int e, int z) -> float4 {
+    // Each thread loads the same LPT padded-tile elements in every plane:
+    // padded column c <-> x0 + c - 1 and row r <-> y0 + r - 1 (periodic), so
+    // column W+1 / row H+1 is the + halo even for a partial tile; columns and
+    // rows past the halo repeat it and stay inside the grid.
+    int toff[LPT], tx_[LPT], ty_[LPT], tsl[LPT];
+#pragma unroll
+    for (int k = 0; k < LPT; ++k) {
+        const int e = tid + k * BX * BY;
         const int r = e / TW, c = e - r * TW;
-        const int cc = (c > W + 1) ? W + 1 : c;  // unused columns: duplicate the halo
-        const int rr = (r > H + 1) ? H + 1 : r;
-        return ld.load(rr * TW + cc, z);
+        const int cc = min(c, W + 1), rr = min(r, H + 1);
+        int xx = x0 + cc - 1, yy = y0 + rr - 1;
+        xx = xx < 0 ? xx + nx : (xx >= nx ? xx - nx : xx);
+        yy = yy < 0 ? yy + ny : (yy >= ny ? yy - ny : yy);
+        tx_[k] = xx;
+        ty_[k] = yy;
+        toff[k] = xx + nx * yy;
+        tsl[k] = (e < TILE) ? e : -1;
+    }
+    const int nxy = nx * ny;
+    auto tile_e = [&](int k, int z) -> float4 {
+        const int cidx = toff[k] + nxy * z;
+        float4 v = __ldg(&a.psi[cidx]);
+        if (a.use_jet) restrict_cell(g, a.jet, tx_[k], ty_[k], z, cidx, v);
+        return v;
     };
+    float4* tflat0 = &tile[0][0][0];
+    float4* tflat1 = &tile[1][0][0];
 
     float4 pre[LPT];
     int cur = 0;
     // prologue: plane z0 into the tile, plane z0+1 into registers
 #pragma unroll
-    for (int k = 0; k < LPT; ++k) {
-        const int e = tid + k * BX * BY;
-        if (e < TILE) tile[0][e / TW][e % TW] = tile_e(e, z0);
-    }
+    for (int k = 0; k < LPT; ++k)
+        if (tsl[k] >= 0) tflat0[tsl[k]] = tile_e(k, z0);
     const int z1 = (z0 + 1 == nz) ? 0 : z0 + 1;
 #pragma unroll
-    for (int k = 0; k < LPT; ++k) {
-        const int e = tid + k * BX * BY;
-        if (e < TILE) pre[k] = tile_e(e, z1);
-    }
+    for (int k = 0; k < LPT; ++k)
+        if (tsl[k] >= 0) pre[k] = tile_e(k, z1);
     float vz_prev = 0.f;
     if constexpr (OP == ST_DIV) {
         float4 pm = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -98,18 +93,15 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
     for (int z = z0; z < zend; ++z) {
         __syncthreads();  // tile[cur] complete; previous iteration's reads done
         const int nxt = cur ^ 1;
+        float4* tn = nxt ? tflat1 : tflat0;
 #pragma unroll
-        for (int k = 0; k < LPT; ++k) {
-            const int e = tid + k * BX * BY;
-            if (e < TILE) tile[nxt][e / TW][e % TW] = pre[k];
-        }
+        for (int k = 0; k < LPT; ++k)
+            if (tsl[k] >= 0) tn[tsl[k]] = pre[k];
         if (z + 1 < zend) {  // prefetch plane z+2
             const int z2 = (z + 2 >= nz) ? z + 2 - nz : z + 2;
 #pragma unroll
-            for (int k = 0; k < LPT; ++k) {
-                const int e = tid + k * BX * BY;
-                if (e < TILE) pre[k] = tile_e(e, z2);
-            }
+            for (int k = 0; k < LPT; ++k)
+                if (tsl[k] >= 0) pre[k] = tile_e(k, z2);
         }
         const float4 c0 = tile[cur][ty + 1][tx + 1];
         if constexpr (OP == ST_DIV) {
@@ -139,10 +131,7 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
                     ay = __fmul_rn(ay, g.dinv[1]);
                     az = __fmul_rn(az, g.dinv[2]);
                 }
-                const long long c = cell(g, x, y, z);
-                a.out[c] = ax;
-                a.out[g.N + c] = ay;
-                a.out[2 * g.N + c] = az;
+                reinterpret_cast<float4*>(a.out)[cell(g, x, y, z)] = make_float4(ax, ay, az, 0.f);
             }
         }
         cur = nxt;

@@ -84,6 +84,33 @@ def test_velocity_one_form_and_div(isfpkg, oracle_mod, L, dims, hbar):
     assert rel(host(isf.velocity), orc.velocity()) < 1e-6
 
 
+def test_one_form_angles_all_quadrants(isfpkg, oracle_mod):
+    """Random (non-smooth) psi: one-form angles cover (-pi, pi]; the kernel's
+    atan2 stays within 2.5e-7 rad of the FP64 oracle (compared modulo 2 pi,
+    so a +-pi branch flip of a value within rounding of the cut is not an error)."""
+    L, dims = (4, 2, 2), (64, 32, 32)
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    rng = np.random.default_rng(12)
+    ph = rng.uniform(-np.pi, np.pi, dims[::-1] + (2,))
+    amp = rng.uniform(0.2, 1.0, dims[::-1] + (2,))
+    psi64 = np.stack([amp[..., 0] * np.cos(ph[..., 0]), amp[..., 0] * np.sin(ph[..., 0]),
+                      amp[..., 1] * np.cos(ph[..., 1]), amp[..., 1] * np.sin(ph[..., 1])], -1)
+    psi64 = psi64.astype(np.float32).astype(np.float64)
+    isfpkg.velocity_one_form(isf, cuda(psi64), 1.0)
+    v = host(isf.velocity)
+    vo = orc.velocity_one_form(psi64, 1.0)
+    d = np.abs((v - vo + np.pi) % (2 * np.pi) - np.pi)
+    # |z| of z = conj(a1) b1 + conj(a2) b2: FP32 rounding of re / im moves the
+    # angle by ~1e-7 / |z| on top of the atan2 error itself
+    zabs = np.zeros_like(vo)
+    c = psi64[..., 0] + 1j * psi64[..., 1], psi64[..., 2] + 1j * psi64[..., 3]
+    for ax, npax in enumerate((2, 1, 0)):
+        zabs[..., ax] = np.abs(np.conj(c[0]) * np.roll(c[0], -1, npax) + np.conj(c[1]) * np.roll(c[1], -1, npax))
+    assert np.abs(vo).max() > 3.1
+    assert (d <= 3e-7 + 3e-7 / zabs).all(), (d * zabs).max()
+
+
 @pytest.mark.parametrize("L,dims", GRIDS)
 def test_poisson_solve(isfpkg, oracle_mod, L, dims):
     isf = isfpkg.ISF(L, dims, HBAR, DT)
@@ -177,6 +204,7 @@ def test_staggered_advect(isfpkg, oracle_mod, L, dims):
     parts = cuda(parts64)
     isfpkg.staggered_advect(parts, isf)
     isf.sync()
+    assert isf.counters()["check_failures"] == 0  # nonzero only in a -DISF_CHECK build
     po, margin = orc.staggered_advect(parts64.copy(), margin=True)
     err = np.abs(host(parts) - po).max(axis=1) / min(L)
     near_face = margin < 1e-4
