@@ -85,7 +85,7 @@ def measured_hbm():
 def traffic_table():
     """dram bytes per launch per site from the committed ncu summary, if any."""
     out = {}
-    p = os.path.join(ROOT, "profiles", "ncu_traffic_c3.md")
+    p = os.path.join(ROOT, "profiles", "ncu_traffic_c3.txt")
     if os.path.exists(p):
         for line in open(p):
             parts = line.strip().split("|")
