@@ -19,7 +19,7 @@
  *     GPUArrays' launches (examples/benchmark.jl:66).  A handle is not
  *     thread-safe; separate handles are independent.
  *   - Grid sizes: each of nx, ny, nz in {8,12,16,24,32,48,64,96,128,192,256,
- *     384,512}, nx a multiple of 16, ny*nz a multiple of 16 (ISF_ERR_INVALID
+ *     384,512}, nx a multiple of 16, ny*nz a multiple of 32 (ISF_ERR_INVALID
  *     otherwise); psi pointers 16-byte aligned, complex arrays 8-byte aligned.
  */
 #ifndef ISF_H

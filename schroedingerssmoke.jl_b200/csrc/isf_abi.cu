@@ -18,7 +18,8 @@ struct isf_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    float2* F = nullptr;     // Poisson spectrum / complex work array, N
+    float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
+    int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
     float* vel = nullptr;    // velocity, float4 (vx, vy, vz, 0) per cell, 4N
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
@@ -149,8 +150,8 @@ bool valid_grid(const int n[3], std::string& why) {
         why = "grid_res[0] must be a multiple of 16";
         return false;
     }
-    if (((long long)n[1] * n[2]) % 16 != 0) {
-        why = "grid_res[1]*grid_res[2] must be a multiple of 16";
+    if (((long long)n[1] * n[2]) % 32 != 0) {
+        why = "grid_res[1]*grid_res[2] must be a multiple of 32";
         return false;
     }
     return true;
@@ -161,6 +162,7 @@ XArgs xargs(isf_handle* h) {
     std::memset(&a, 0, sizeof(a));
     a.g = h->g;
     a.F = h->F;
+    a.wp = h->wp;
     return a;
 }
 
@@ -169,6 +171,16 @@ YZArgs yzargs(isf_handle* h, void* data, int axis) {
     a.g = h->g;
     a.data = data;
     a.axis = axis;
+    a.row = h->g.n[0];
+    a.kx_valid = h->g.n[0];
+    return a;
+}
+
+// y / z passes over the half spectrum of the Poisson solve
+YZArgs yzhalf(isf_handle* h, int axis) {
+    YZArgs a = yzargs(h, h->F, axis);
+    a.row = h->wp;
+    a.kx_valid = h->g.n[0] / 2 + 1;
     return a;
 }
 
@@ -216,11 +228,11 @@ int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
         xa.use_jet = 1;
     }
     ISF_LAUNCH(h, launch_stencil(ST_DIV, sa, h->stream), "projection div");
-    ISF_LAUNCH(h, launch_xpass(X_REAL_FWD, xa, h->stream), "projection x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "projection y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "projection z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "projection y inv");
-    ISF_LAUNCH(h, launch_xpass(X_GAUGE_INV, xa, h->stream), "projection x inv + gauge");
+    ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "projection x fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "projection y fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "projection z fac");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "projection y inv");
+    ISF_LAUNCH(h, launch_xreal(XR_INV_GAUGE, xa, h->stream), "projection x inv + gauge");
     return ISF_OK;
 }
 
@@ -275,8 +287,10 @@ int isf_create(const isf_params* p, isf_handle** out) {
         g.dinv[a] = 1.0f / g.d[a];                                                // benchmark.jl:62
         int ex = 0;
         g.d_pow2[a] = (std::frexp(g.d[a], &ex) == 0.5f) ? 1 : 0;
+        g.feps[a] = 4.0f * (std::nextafter((float)g.n[a], 1e30f) - (float)g.n[a]);
     }
     g.N = (long long)g.n[0] * g.n[1] * g.n[2];
+    h->wp = ((g.n[0] / 2 + 1 + 15) / 16) * 16;
     g.hbar = p->hbar;
     g.dt = p->dt;
     g.invN = 1.0 / (double)g.N;
@@ -338,6 +352,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float4) * g.N);
+    if (e == cudaSuccess) e = cudaMemset(h->F, 0, sizeof(float2) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
     char* base = reinterpret_cast<char*>(h->tables);
     off = 0;
@@ -574,11 +589,11 @@ int isf_poisson_solve(isf_handle* h, const float* f, float* q) {
     XArgs xa = xargs(h);
     xa.rin = f;
     xa.rout = q;
-    ISF_LAUNCH(h, launch_xpass(X_REAL_FWD, xa, h->stream), "poisson x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzargs(h, h->F, 1), h->stream), "poisson y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzargs(h, h->F, 2), h->stream), "poisson z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzargs(h, h->F, 1), h->stream), "poisson y inv");
-    ISF_LAUNCH(h, launch_xpass(X_REAL_INV, xa, h->stream), "poisson x inv");
+    ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "poisson x fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "poisson y fwd");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "poisson z fac");
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "poisson y inv");
+    ISF_LAUNCH(h, launch_xreal(XR_INV_REAL, xa, h->stream), "poisson x inv");
     return ISF_OK;
 }
 

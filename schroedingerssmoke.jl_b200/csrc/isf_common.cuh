@@ -21,6 +21,7 @@ struct Grid {
     float inv_d2[3];   // inv.(d .^ 2f0)                    parallel.jl:150
     float dinv[3];     // inv.(d)                           benchmark.jl:62
     int d_pow2[3];     // d is a power of two: p * dinv == p / d exactly
+    float feps[3];     // 4 ulp of n (a bound on 4 ulp of p / d for p <= L)
     float hbar, dt;
     const float2* tw[3];    // tw[a][j] = exp(-2 pi i j / n[a]) rounded from double
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))

@@ -13,10 +13,12 @@
 // last stage scatters straight to the caller's sink, so only the stage
 // boundaries in between go through shared memory: one [N][C] tile per CTA,
 // in place (a barrier after every gather and after every scatter).  The
-// tile stores element (j, q) of pencil q at j*C + (q ^ swz(j)); the XOR
-// swizzle keeps row-wise (y/z passes: lanes over q) and column-wise (x pass:
-// lanes over j, including the stride-R scatter of the first stage) accesses
-// free of bank conflicts, since C * sizeof(T) is 128 bytes.
+// tile stores element (j, q) of pencil q at j*C + (q ^ ((j ^ (j >> 3)) mod C)):
+// row-wise accesses (y/z passes: lanes over q) are conflict free for any
+// swizzle since C * sizeof(T) is 128 bytes; this one also keeps the
+// column-wise stage accesses of the x pass (lanes over j, strides 1, R and
+// the grouped p-strides) within 1.04 x the ideal wavefront count for every
+// radix plan (simulated per quarter / half warp for 16- / 8-byte elements).
 //
 // Forward transforms use S = -1 (unnormalised), inverse S = +1 (the 1/N of
 // the reference's ifft is folded into the spectral multiply by the callers).
@@ -29,9 +31,8 @@ namespace isf {
 
 template <int C>
 __device__ __forceinline__ int sidx(int j, int q) {
-    constexpr int LOG = (C == 8) ? 3 : 4;
     static_assert(C == 8 || C == 16, "tile width");
-    return j * C + (q ^ ((j ^ (j >> LOG)) & (C - 1)));
+    return j * C + (q ^ ((j ^ (j >> 3)) & (C - 1)));
 }
 
 // --------------------------------------------------------------- radix DFTs

@@ -13,6 +13,7 @@ struct YZArgs;
 bool supported_len(int n);
 
 cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s);
+cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_psi(int op, const YZArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s);
 

@@ -3,8 +3,9 @@
 // A 3D transform is three axis passes over the array in HBM; each pass is in
 // place and moves every element once (read + write).  Fusions:
 //   Schroedinger step  x fwd | y fwd | z fwd * mask/N, z inv | y inv | x inv + normalize
-//   Poisson solve      x fwd of the real divergence f | y fwd | z fwd * fac/N, z inv
-//                      | y inv | x inv + gauge of psi (+ the nozzle restriction)
+//   Poisson solve      real-to-complex x fwd of the divergence f | y fwd on the half
+//                      spectrum | z fwd * fac/N, z inv | y inv | complex-to-real x inv
+//                      + gauge of psi (+ the nozzle restriction)
 // so the reference's split/merge broadcasts (parallel.jl:179-180, 185), the
 // complex(f) copy (:169), the mask / fac multiplies (:171, :182-183) and the
 // gauge broadcast (:159) never touch HBM on their own.
@@ -23,11 +24,8 @@ enum XOp {
     X_PSI_FWD = 0,       // psi rows, forward
     X_PSI_INV = 1,       // psi rows, inverse
     X_PSI_INV_NORM = 2,  // psi rows, inverse, then normalize_psi
-    X_C_FWD = 3,         // complex work array F, forward
-    X_C_INV = 4,         // complex work array F, inverse
-    X_GAUGE_INV = 6,     // F inverse -> q = Re; psi = gauge(psi (restricted), q)
-    X_REAL_FWD = 7,      // real input array -> F, forward
-    X_REAL_INV = 8,      // F inverse -> real part to a real output array
+    X_C_FWD = 3,         // complex array, forward
+    X_C_INV = 4,         // complex array, inverse
 };
 
 struct XArgs {
@@ -38,6 +36,7 @@ struct XArgs {
     float* rout;
     JetArgs jet;
     int use_jet;
+    int wp;  // row stride (complex elements) of the half spectrum of real data
 };
 
 template <int OP>
@@ -45,7 +44,7 @@ struct XTraits {
     static constexpr bool psi_elems = (OP == X_PSI_FWD || OP == X_PSI_INV || OP == X_PSI_INV_NORM);
     using T = typename std::conditional<psi_elems, float4, float2>::type;
     static constexpr int C = 128 / (int)sizeof(T);
-    static constexpr int S = (OP == X_PSI_FWD || OP == X_C_FWD || OP == X_REAL_FWD) ? -1 : +1;
+    static constexpr int S = (OP == X_PSI_FWD || OP == X_C_FWD) ? -1 : +1;
 };
 
 template <int N, int OP>
@@ -72,8 +71,6 @@ __global__ void __launch_bounds__(XShape<N, OP>::BLK) k_xpass(XArgs a) {
     auto src = [&](int j) -> T {
         if constexpr (Tr::psi_elems) {
             return a.psi[rb + j];
-        } else if constexpr (OP == X_REAL_FWD) {
-            return make_float2(__ldg(&a.rin[rb + j]), 0.f);
         } else {
             return a.F[rb + j];
         }
@@ -83,21 +80,90 @@ __global__ void __launch_bounds__(XShape<N, OP>::BLK) k_xpass(XArgs a) {
             a.psi[rb + j] = v;
         } else if constexpr (OP == X_PSI_INV_NORM) {
             a.psi[rb + j] = normalize4(v);
-        } else if constexpr (OP == X_C_FWD || OP == X_C_INV || OP == X_REAL_FWD) {
-            a.F[rb + j] = v;
-        } else if constexpr (OP == X_REAL_INV) {
-            a.rout[rb + j] = v.x;
         } else {
-            static_assert(OP == X_GAUGE_INV, "unhandled x-pass op");
-            float4 p = a.psi[rb + j];
-            if (a.use_jet) {
-                const int ny = a.g.n[1];
-                restrict_cell(a.g, a.jet, j, (int)(row % ny), (int)(row / ny), rb + j, p);
-            }
-            a.psi[rb + j] = gauge4(p, v.x);
+            static_assert(OP == X_C_FWD || OP == X_C_INV, "unhandled x-pass op");
+            a.F[rb + j] = v;
         }
     };
     Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst);
+}
+
+// ------------------------------------------- x pass of real data (Poisson)
+// Two real rows r0 = 2m, r1 = 2m+1 travel as one complex pencil a + i b.
+//   XR_FWD        f rows -> half spectra A[k], B[k], k = 0..N/2, with
+//                 A = (Z_k + conj Z_{N-k}) / 2 and B = (Z_k - conj Z_{N-k}) / 2i
+//   XR_INV_GAUGE  Z_j = A_j + i B_j (Hermitian extension for j > N/2) ->
+//                 inverse -> q rows (Re, Im) -> psi = gauge(psi (restricted), q)
+//   XR_INV_REAL   the same inverse, q rows to a real output array
+// The half spectrum of row r starts at F + r * wp (wp >= N/2 + 1, padded to
+// whole 16-column tiles for the y / z passes).
+enum XROp { XR_FWD = 0, XR_INV_GAUGE = 1, XR_INV_REAL = 2 };
+
+template <int N>
+struct XRShape {
+    static constexpr int C = 16;
+    static constexpr int NT = Plan<N>::NT;
+    static constexpr int BLK = C * NT;
+    static constexpr size_t SMEM = (size_t)N * C * sizeof(float2);
+};
+
+template <int N, int OP>
+__global__ void __launch_bounds__(XRShape<N>::BLK) k_xreal(XArgs a) {
+    using T = float2;
+    constexpr int C = 16;
+    constexpr int NT = Plan<N>::NT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* sm = reinterpret_cast<T*>(smraw);
+    const int t = threadIdx.x % NT, q = threadIdx.x / NT;
+    const long long r0 = 2 * ((long long)blockIdx.x * C + q);
+    const int wp = a.wp;
+    T x[Plan<N>::EMAX];
+    if constexpr (OP == XR_FWD) {
+        const float* __restrict__ f0 = a.rin + r0 * N;
+        const float* __restrict__ f1 = f0 + N;
+        auto src = [&](int j) -> T { return make_float2(__ldg(&f0[j]), __ldg(&f1[j])); };
+        auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
+        Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst);
+        __syncthreads();
+        float2* __restrict__ A = a.F + r0 * wp;
+        float2* __restrict__ B = A + wp;
+#pragma unroll 1
+        for (int k = t; k <= N / 2; k += NT) {
+            const float2 zk = sm[sidx<C>(k, q)];
+            const float2 zn = sm[sidx<C>(k == 0 ? 0 : N - k, q)];
+            A[k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+            B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+        }
+    } else {
+        const float2* __restrict__ A = a.F + r0 * wp;
+        const float2* __restrict__ B = A + wp;
+        auto src = [&](int j) -> T {
+            if (j <= N / 2) {
+                const float2 u = A[j], v = B[j];
+                return make_float2(u.x - v.y, u.y + v.x);
+            }
+            const float2 u = A[N - j], v = B[N - j];
+            return make_float2(u.x + v.y, v.x - u.y);
+        };
+        const long long b0 = r0 * N, b1 = b0 + N;
+        auto dst = [&](int j, const T& v) {
+            if constexpr (OP == XR_INV_REAL) {
+                a.rout[b0 + j] = v.x;
+                a.rout[b1 + j] = v.y;
+            } else {
+                static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
+                float4 p0 = a.psi[b0 + j], p1 = a.psi[b1 + j];
+                if (a.use_jet) {
+                    const int ny = a.g.n[1];
+                    restrict_cell(a.g, a.jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
+                    restrict_cell(a.g, a.jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
+                }
+                a.psi[b0 + j] = gauge4(p0, v.x);
+                a.psi[b1 + j] = gauge4(p1, v.y);
+            }
+        };
+        Plan<N>::template run<C, +1, false>(x, t, q, sm, a.g.tw[0], src, dst);
+    }
 }
 
 // -------------------------------------------------------------- y / z pass
@@ -111,7 +177,9 @@ enum YZOp {
 struct YZArgs {
     Grid g;
     void* data;
-    int axis;  // 1 (y) or 2 (z)
+    int axis;      // 1 (y) or 2 (z)
+    int row;       // elements per x row of data (nx, or the padded half-spectrum width)
+    int kx_valid;  // columns holding spectrum data; the others are padding
 };
 
 template <int N, class T>
@@ -120,6 +188,8 @@ struct YZShape {
     static constexpr int NT = Plan<N>::NT;
     static constexpr int BLK = C * NT;
     static constexpr size_t SMEM = (size_t)N * C * sizeof(T);
+    // at least 768 resident threads per SM (caps registers at 85)
+    static constexpr int MINB = (768 / BLK) > 1 ? (768 / BLK) : 1;
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
@@ -127,21 +197,21 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 }
 
 template <int N, class T, int OP>
-__global__ void __launch_bounds__(YZShape<N, T>::BLK) k_yzpass(YZArgs a) {
+__global__ void __launch_bounds__(YZShape<N, T>::BLK, YZShape<N, T>::MINB) k_yzpass(YZArgs a) {
     constexpr int C = YZShape<N, T>::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);
     const int q = threadIdx.x % C, t = threadIdx.x / C;
-    const int nx = a.g.n[0], ny = a.g.n[1];
+    const int rl = a.row, ny = a.g.n[1];
     const int x0 = blockIdx.x * C;
     const int o = blockIdx.y;
     long long stride, base;
     if (a.axis == 1) {
-        stride = nx;
-        base = x0 + (long long)o * nx * ny;
+        stride = rl;
+        base = x0 + (long long)o * rl * ny;
     } else {
-        stride = (long long)nx * ny;
-        base = x0 + (long long)o * nx;
+        stride = (long long)rl * ny;
+        base = x0 + (long long)o * rl;
     }
     T* __restrict__ data = reinterpret_cast<T*>(a.data);
     const float2* tw = a.g.tw[a.axis];
@@ -163,24 +233,26 @@ __global__ void __launch_bounds__(YZShape<N, T>::BLK) k_yzpass(YZArgs a) {
             // exp(i (th_x + th_y + th_z)) / N in double, rounded to float: the
             // reference's Float32(exp(i lambda dt / 2)) (parallel.jl:58-62) up
             // to the double rounding of the product
-            const double2 cxo = zmul(a.g.mtab[0][kx], a.g.mtab[other][o]);
+            double2 cxo = zmul(a.g.mtab[0][kx], a.g.mtab[other][o]);
+            cxo.x *= a.g.invN;
+            cxo.y *= a.g.invN;
             const double2* __restrict__ mt = a.g.mtab[a.axis];
-            const double invN = a.g.invN;
             auto mdst = [&](int j, const T& v) {
-                const double2 m = zmul(cxo, mt[j]);
-                sm[sidx<C>(j, q)] = cmul(v, make_float2((float)(m.x * invN), (float)(m.y * invN)));
+                const double2 m = zmul(cxo, __ldg(&mt[j]));
+                sm[sidx<C>(j, q)] = cmul(v, make_float2((float)m.x, (float)m.y));
             };
             Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, mdst);
         } else {
             static_assert(OP == YZ_FAC, "unhandled y/z op");
             // fac(k)/N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
             // (parallel.jl:53-55, 63)
-            const double dxo = a.g.s2[0][kx] + a.g.s2[other][o];
+            const bool pad = kx >= a.kx_valid;  // padding column of a half spectrum
+            const double dxo = (pad ? 0.0 : a.g.s2[0][kx]) + a.g.s2[other][o];
             const bool zero_line = (kx == 0) && (o == 0);
             const double* __restrict__ s2 = a.g.s2[a.axis];
             const double sc = -0.25 * a.g.invN;
             auto fdst = [&](int j, const T& v) {
-                const float f = (zero_line && j == 0) ? 0.f : (float)(sc / (dxo + s2[j]));
+                const float f = (pad || (zero_line && j == 0)) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2[j])));
                 sm[sidx<C>(j, q)] = cscale(v, f);
             };
             Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, fdst);

@@ -75,9 +75,33 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
         case X_PSI_INV_NORM: return launch_x_op<X_PSI_INV_NORM>(a, s);
         case X_C_FWD: return launch_x_op<X_C_FWD>(a, s);
         case X_C_INV: return launch_x_op<X_C_INV>(a, s);
-        case X_GAUGE_INV: return launch_x_op<X_GAUGE_INV>(a, s);
-        case X_REAL_FWD: return launch_x_op<X_REAL_FWD>(a, s);
-        case X_REAL_INV: return launch_x_op<X_REAL_INV>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int N, int OP>
+static cudaError_t launch_xr_n(const XArgs& a, cudaStream_t s) {
+    using Sh = XRShape<N>;
+    static std::atomic<unsigned long long> done{0};
+    cudaError_t e = ensure_smem(k_xreal<N, OP>, Sh::SMEM, done);
+    if (e != cudaSuccess) return e;
+    const long long rows = (long long)a.g.n[1] * a.g.n[2];
+    k_xreal<N, OP><<<(unsigned)(rows / (2 * Sh::C)), Sh::BLK, Sh::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int OP>
+static cudaError_t launch_xr_op(const XArgs& a, cudaStream_t s) {
+#define ISF_XR(NN) return launch_xr_n<NN, OP>(a, s)
+    ISF_SIZE_SWITCH(a.g.n[0], ISF_XR)
+#undef ISF_XR
+}
+
+cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s) {
+    switch (op) {
+        case XR_FWD: return launch_xr_op<XR_FWD>(a, s);
+        case XR_INV_GAUGE: return launch_xr_op<XR_INV_GAUGE>(a, s);
+        case XR_INV_REAL: return launch_xr_op<XR_INV_REAL>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -89,7 +113,7 @@ static cudaError_t launch_yz_n(const YZArgs& a, cudaStream_t s) {
     cudaError_t e = ensure_smem(k_yzpass<N, T, OP>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const int other = (a.axis == 1) ? a.g.n[2] : a.g.n[1];
-    dim3 grid((unsigned)(a.g.n[0] / Sh::C), (unsigned)other);
+    dim3 grid((unsigned)(a.row / Sh::C), (unsigned)other);
     k_yzpass<N, T, OP><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
     return cudaGetLastError();
 }

@@ -79,11 +79,6 @@ __device__ __forceinline__ float jl_mod_box(float x, float L) {
     return r;
 }
 
-// staggered_velocity (parallel.jl:219-246) on the handle's velocity
-// (float4 (vx, vy, vz, 0) per cell).  Interpolation weights are the
-// reference's unnormalised w = p - (i-1) d.  An index that rounds to n (p
-// rounded up to L by mod) is clamped to the last cell and counted.
-// POW2: every d is a power of two, so p * (1/d) == p / d exactly.
 // Gather of one velocity cell.  With -DISF_CHECK (debug builds) every index
 // is validated; a bad one is recorded in chk[0..1] (count, first index) and
 // replaced by cell 0 instead of being read.
@@ -107,26 +102,48 @@ __device__ __forceinline__ float4 vload(const Grid& g, const float4* __restrict_
     return __ldg(&v[c]);
 }
 
+// floor(fl(p / d)) for p in [0, L]: with d a power of two p * (1/d) is exact;
+// otherwise p * fl(1/d) differs from fl(p / d) by at most 3 ulp(p / d), so
+// when it lies more than eps = 4 ulp(n) from an integer both have the same
+// floor, and near an integer the IEEE quotient decides.
+template <bool POW2>
+__device__ __forceinline__ int cell_floor(float p, float dinv, float d, float eps) {
+    const float q1 = p * dinv;
+    if (POW2) return __float2int_rd(q1);
+    const float f1 = floorf(q1);
+    const float fr = q1 - f1;
+    return (fr > eps && fr < 1.f - eps) ? (int)f1 : __float2int_rd(__fdiv_rn(p, d));
+}
+
+// staggered_velocity (parallel.jl:219-246) on the handle's velocity
+// (float4 (vx, vy, vz, 0) per cell).  Interpolation weights are the
+// reference's unnormalised w = p - (i-1) d.  An index that rounds to n (p
+// rounded up to L by mod) is clamped to the last cell and counted.
 template <bool POW2>
 __device__ __forceinline__ float3 stag_vel(const Grid& g, const float4* __restrict__ v, float3 pt,
                                            unsigned& clamps, unsigned long long* chk) {
-    const float P[3] = {pt.x, pt.y, pt.z};
+    float P[3] = {pt.x, pt.y, pt.z};
+    // mod.(point, ph_size): identity for points inside the box (the common case)
+    const bool inbox = (pt.x >= 0.f && pt.x < g.L[0]) && (pt.y >= 0.f && pt.y < g.L[1]) &&
+                       (pt.z >= 0.f && pt.z < g.L[2]);
+    if (!inbox) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], g.L[a]);
+    }
     int i[3], ip[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float p = jl_mod_box(P[a], g.L[a]);
-        const float qd = POW2 ? p * g.dinv[a] : __fdiv_rn(p, g.d[a]);
         const int nm = g.n[a] - 1;
-        int ii = __float2int_rd(qd);  // UInt32(floor(p / d))
-        if (ii > nm) {
+        int ii = cell_floor<POW2>(P[a], g.dinv[a], g.d[a], g.feps[a]);
+        if (ii > nm) {  // mod rounded up to L
             ii = nm;
             ++clamps;
         }
-        if (ii < 0) ii = 0;
+        ii = max(ii, 0);
         i[a] = ii;
         ip[a] = (ii < nm) ? ii + 1 : 0;  // mod(i, res) + 1 (periodic +1 neighbour)
-        w[a] = __fsub_rn(p, __fmul_rn((float)ii, g.d[a]));
+        w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, g.d[a]));
     }
     const int nx = g.n[0], nxy = g.n[0] * g.n[1];
     const int ry0 = i[1] * nx, ry1 = ip[1] * nx, rz0 = i[2] * nxy, rz1 = ip[2] * nxy;
