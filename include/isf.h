@@ -146,7 +146,7 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
 /* First n (<= 16) counters of the advections since the last reset: [0] clamp
  * events (staggered_velocity index rounded to n+1), [1] live particles; in a
  * bounds-checking build (-DISF_CHECK) [2] rejected gather indices, [3] the
- * first of them and [4..11] its cell indices, +1 neighbours and strides.
+ * first of them and [4..11] its cell indices, two neighbour indices and strides.
  * Synchronises the handle's stream. */
 ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);
 

@@ -18,14 +18,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 # ISF_CHECK=1 builds the bounds-checking debug variant libisf_check.so
 CHECK = os.environ.get("ISF_CHECK", "0") == "1"
-BUILD = os.path.join(HERE, "_build_check" if CHECK else "_build")
-LIB = os.path.join(HERE, "libisf_check.so" if CHECK else "libisf.so")
+BUILD = os.environ.get("ISF_BUILD_DIR") or os.path.join(HERE, "_build_check" if CHECK else "_build")
+LIB = os.environ.get("ISF_LIB_OUT") or os.path.join(HERE, "libisf_check.so" if CHECK else "libisf.so")
+# extra nvcc flags, e.g. -DISF_ST_SZ=16 to build a tuning variant elsewhere
+EXTRA = os.environ.get("ISF_EXTRA_FLAGS", "").split()
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-         "--expt-relaxed-constexpr", "-I", INCLUDE] + (["-DISF_CHECK"] if CHECK else [])
+         "--expt-relaxed-constexpr", "-I", INCLUDE] + (["-DISF_CHECK"] if CHECK else []) + EXTRA
 
 
 def _headers():

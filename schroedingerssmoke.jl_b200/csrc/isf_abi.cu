@@ -21,7 +21,7 @@ struct isf_handle {
     float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
     int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
-    float* vel = nullptr;    // velocity, float4 (vx, vy, vz, 0) per cell, 4N
+    float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
     unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
     unsigned long long launches = 0;         // kernels launched by this handle
@@ -291,6 +291,9 @@ int isf_create(const isf_params* p, isf_handle** out) {
     }
     g.N = (long long)g.n[0] * g.n[1] * g.n[2];
     h->wp = ((g.n[0] / 2 + 1 + 15) / 16) * 16;
+    g.pnx = g.n[0] + 1;
+    g.pnxy = (g.n[0] + 1) * (g.n[1] + 1);
+    g.NP = (long long)g.pnxy * (g.n[2] + 1);
     g.hbar = p->hbar;
     g.dt = p->dt;
     g.invN = 1.0 / (double)g.N;
@@ -343,7 +346,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
         h->own_stream = true;
     }
     if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess || cudaMalloc(&h->f, sizeof(float) * g.N) != cudaSuccess ||
-        cudaMalloc(&h->vel, sizeof(float4) * g.N) != cudaSuccess ||
+        cudaMalloc(&h->vel, sizeof(float) * 3 * g.NP) != cudaSuccess ||
         cudaMalloc(&h->tables, total) != cudaSuccess ||
         cudaMalloc(&h->counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
@@ -351,7 +354,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     }
     e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float4) * g.N);
+    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float) * 3 * g.NP);
     if (e == cudaSuccess) e = cudaMemset(h->F, 0, sizeof(float2) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
     char* base = reinterpret_cast<char*>(h->tables);

@@ -4,7 +4,10 @@
 //   cell index  c = x + nx*(y + ny*z)  (column-major, x fastest)
 //   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
 //               == NTuple{2,ComplexF32} of src/parallel.jl
-//   velocity    float4 (vx, vy, vz, 0) per cell (internal to the handle)
+//   velocity    three planes vx | vy | vz (internal to the handle), each
+//               (nx+1) x (ny+1) x (nz+1) with a periodic copy of the x = 0,
+//               y = 0 and z = 0 faces at x = nx, y = ny, z = nz, so the +1
+//               neighbour of any cell is a fixed offset (+1, +pnx, +pnxy)
 //   F           float2 per cell: the Poisson spectrum work array
 //   particles   float3 per slot (AoS), dead slot = (-1,-1,-1)
 #pragma once
@@ -27,7 +30,29 @@ struct Grid {
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))
     const double* s2[3];    // (sin(pi k / n_a) / d_a)^2 in double
     double invN;            // 1 / N
+    int pnx, pnxy;          // strides of the padded velocity planes: nx+1, (nx+1)(ny+1)
+    long long NP;           // cells of one padded velocity plane
 };
+
+// index of cell (x, y, z), 0 <= x <= nx etc., in a padded velocity plane
+__host__ __device__ __forceinline__ int pcell(const Grid& g, int x, int y, int z) {
+    return x + g.pnx * y + g.pnxy * z;
+}
+
+// store v at cell (x, y, z) of a padded velocity plane and at its periodic
+// copies on the +faces (only cells on a low face have copies)
+__device__ __forceinline__ void pstore(const Grid& g, float* __restrict__ plane, int x, int y, int z, float v) {
+    plane[pcell(g, x, y, z)] = v;
+    if ((x == 0) | (y == 0) | (z == 0)) {
+        const int X = (x == 0) ? g.n[0] : x, Y = (y == 0) ? g.n[1] : y, Z = (z == 0) ? g.n[2] : z;
+        // every combination of original / copied coordinate except the original itself
+        for (int m = 1; m < 8; ++m) {
+            const int xx = (m & 1) ? X : x, yy = (m & 2) ? Y : y, zz = (m & 4) ? Z : z;
+            if ((m & 1 && x != 0) || (m & 2 && y != 0) || (m & 4 && z != 0)) continue;
+            plane[pcell(g, xx, yy, zz)] = v;
+        }
+    }
+}
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }

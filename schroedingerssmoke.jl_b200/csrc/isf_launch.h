@@ -22,7 +22,7 @@ enum StOp { ST_DIV = 0, ST_VEL = 1 };
 struct StencilArgs {
     Grid g;
     const float4* psi;
-    float* out;  // ST_DIV: f[N]; ST_VEL: float4 (vx, vy, vz, 0) per cell
+    float* out;  // ST_DIV: f[N]; ST_VEL: padded vx | vy | vz planes (3 NP)
     JetArgs jet;
     int use_jet;
     float hbar;

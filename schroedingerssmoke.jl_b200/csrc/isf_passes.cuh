@@ -182,14 +182,23 @@ struct YZArgs {
     int kx_valid;  // columns holding spectrum data; the others are padding
 };
 
-template <int N, class T>
+// minimum resident threads per SM the y / z passes are compiled for (caps
+// their registers); the spectral ones hold the FP64 symbol products as well
+#ifndef ISF_YZ_MIN_THREADS
+#define ISF_YZ_MIN_THREADS 768
+#endif
+#ifndef ISF_YZ_SPECTRAL_MIN_THREADS
+#define ISF_YZ_SPECTRAL_MIN_THREADS 768
+#endif
+
+template <int N, class T, int OP = 0>
 struct YZShape {
     static constexpr int C = 128 / (int)sizeof(T);
     static constexpr int NT = Plan<N>::NT;
     static constexpr int BLK = C * NT;
     static constexpr size_t SMEM = (size_t)N * C * sizeof(T);
-    // at least 768 resident threads per SM (caps registers at 85)
-    static constexpr int MINB = (768 / BLK) > 1 ? (768 / BLK) : 1;
+    static constexpr int MINT = (OP >= 2) ? ISF_YZ_SPECTRAL_MIN_THREADS : ISF_YZ_MIN_THREADS;
+    static constexpr int MINB = (MINT / BLK) > 1 ? (MINT / BLK) : 1;
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
@@ -197,7 +206,7 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 }
 
 template <int N, class T, int OP>
-__global__ void __launch_bounds__(YZShape<N, T>::BLK, YZShape<N, T>::MINB) k_yzpass(YZArgs a) {
+__global__ void __launch_bounds__(YZShape<N, T, OP>::BLK, YZShape<N, T, OP>::MINB) k_yzpass(YZArgs a) {
     constexpr int C = YZShape<N, T>::C;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* sm = reinterpret_cast<T*>(smraw);

@@ -79,13 +79,13 @@ __device__ __forceinline__ float jl_mod_box(float x, float L) {
     return r;
 }
 
-// Gather of one velocity cell.  With -DISF_CHECK (debug builds) every index
-// is validated; a bad one is recorded in chk[0..1] (count, first index) and
-// replaced by cell 0 instead of being read.
-__device__ __forceinline__ float4 vload(const Grid& g, const float4* __restrict__ v, int c,
-                                        unsigned long long* chk, const int* ctx) {
+// Gather of one velocity component.  With -DISF_CHECK (debug builds) every
+// index is validated; a bad one is recorded in chk[0..9] (count, first index,
+// its cell indices, +1 neighbours and strides) and replaced by cell 0.
+__device__ __forceinline__ float vload(const Grid& g, const float* __restrict__ v, int c,
+                                       unsigned long long* chk, const int* ctx) {
 #ifdef ISF_CHECK
-    if (c < 0 || (long long)c >= g.N) {
+    if (c < 0 || (long long)c >= g.NP) {
         if (chk) {
             if (atomicAdd(&chk[0], 1ull) == 0) {
                 chk[1] = (unsigned long long)(unsigned)c;
@@ -115,12 +115,11 @@ __device__ __forceinline__ int cell_floor(float p, float dinv, float d, float ep
     return (fr > eps && fr < 1.f - eps) ? (int)f1 : __float2int_rd(__fdiv_rn(p, d));
 }
 
-// staggered_velocity (parallel.jl:219-246) on the handle's velocity
-// (float4 (vx, vy, vz, 0) per cell).  Interpolation weights are the
+// staggered_velocity (parallel.jl:219-246) on the handle's padded velocity planes.  Interpolation weights are the
 // reference's unnormalised w = p - (i-1) d.  An index that rounds to n (p
 // rounded up to L by mod) is clamped to the last cell and counted.
 template <bool POW2>
-__device__ __forceinline__ float3 stag_vel(const Grid& g, const float4* __restrict__ v, float3 pt,
+__device__ __forceinline__ float3 stag_vel(const Grid& g, const float* __restrict__ v, float3 pt,
                                            unsigned& clamps, unsigned long long* chk) {
     float P[3] = {pt.x, pt.y, pt.z};
     // mod.(point, ph_size): identity for points inside the box (the common case)
@@ -130,43 +129,44 @@ __device__ __forceinline__ float3 stag_vel(const Grid& g, const float4* __restri
 #pragma unroll
         for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], g.L[a]);
     }
-    int i[3], ip[3];
+    int i[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int nm = g.n[a] - 1;
         int ii = cell_floor<POW2>(P[a], g.dinv[a], g.d[a], g.feps[a]);
-        if (ii > nm) {  // mod rounded up to L
-            ii = nm;
-            ++clamps;
-        }
-        ii = max(ii, 0);
+        clamps += (ii > nm);  // mod rounded up to L
+        ii = max(min(ii, nm), 0);
         i[a] = ii;
-        ip[a] = (ii < nm) ? ii + 1 : 0;  // mod(i, res) + 1 (periodic +1 neighbour)
         w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, g.d[a]));
     }
-    const int nx = g.n[0], nxy = g.n[0] * g.n[1];
-    const int ry0 = i[1] * nx, ry1 = ip[1] * nx, rz0 = i[2] * nxy, rz1 = ip[2] * nxy;
-    const int c000 = i[0] + ry0 + rz0;
-    const int c100 = ip[0] + ry0 + rz0, c010 = i[0] + ry1 + rz0, c001 = i[0] + ry0 + rz1;
-    const int c011 = i[0] + ry1 + rz1, c101 = ip[0] + ry0 + rz1, c110 = ip[0] + ry1 + rz0;
+    // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell
+    const int sy = g.pnx, sz = g.pnxy;
+    const int c000 = i[0] + sy * i[1] + sz * i[2];
+    const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
+    const int c011 = c010 + sz, c101 = c100 + sz, c110 = c100 + sy;
 #ifdef ISF_CHECK
-    const int ctx[8] = {i[0], i[1], i[2], ip[0], ip[1], ip[2], nx, nxy};
+    const int ctx[8] = {i[0], i[1], i[2], c000, c011, c101, sy, sz};
 #else
     const int* ctx = nullptr;
 #endif
-    const float4 v000 = vload(g, v, c000, chk, ctx);
-    const float4 v100 = vload(g, v, c100, chk, ctx);    // pxp
-    const float4 v010 = vload(g, v, c010, chk, ctx);    // pyp
-    const float4 v001 = vload(g, v, c001, chk, ctx);    // pzp
-    const float x11 = vload(g, v, c011, chk, ctx).x;    // velocity[i, jp, kp][1]
-    const float y11 = vload(g, v, c101, chk, ctx).y;    // velocity[ip, j, kp][2]
-    const float z11 = vload(g, v, c110, chk, ctx).z;    // velocity[ip, jp, k][3]
+    // 12 scalar gathers: a warp of cell-sorted particles mostly reads one
+    // address per load, which the L1 serves as one broadcast wavefront
+    const float* __restrict__ vx = v;
+    const float* __restrict__ vy = v + g.NP;
+    const float* __restrict__ vz = v + 2 * g.NP;
+    const float x00 = vload(g, vx, c000, chk, ctx), x10 = vload(g, vx, c010, chk, ctx);
+    const float x01 = vload(g, vx, c001, chk, ctx), x11 = vload(g, vx, c011, chk, ctx);
+    const float y00 = vload(g, vy, c000, chk, ctx), y10 = vload(g, vy, c100, chk, ctx);
+    const float y01 = vload(g, vy, c001, chk, ctx), y11 = vload(g, vy, c101, chk, ctx);
+    const float z00 = vload(g, vz, c000, chk, ctx), z10 = vload(g, vz, c100, chk, ctx);
+    const float z01 = vload(g, vz, c010, chk, ctx), z11 = vload(g, vz, c110, chk, ctx);
     const float wx = w[0], wy = w[1], wz = w[2];
     float3 u;
-    u.x = (1.f - wz) * ((1.f - wy) * v000.x + wy * v010.x) + wz * ((1.f - wy) * v001.x + wy * x11);
-    u.y = (1.f - wz) * ((1.f - wx) * v000.y + wx * v100.y) + wz * ((1.f - wx) * v001.y + wx * y11);
-    u.z = (1.f - wy) * ((1.f - wx) * v000.z + wx * v100.z) + wy * ((1.f - wx) * v010.z + wx * z11);
+    // u_x bilinear in (y, z), u_y in (x, z), u_z in (x, y) (parallel.jl:230-245)
+    u.x = (1.f - wz) * ((1.f - wy) * x00 + wy * x10) + wz * ((1.f - wy) * x01 + wy * x11);
+    u.y = (1.f - wz) * ((1.f - wx) * y00 + wx * y10) + wz * ((1.f - wx) * y01 + wx * y11);
+    u.z = (1.f - wy) * ((1.f - wx) * z00 + wx * z10) + wy * ((1.f - wx) * z01 + wx * z11);
     return u;
 }
 
@@ -175,7 +175,7 @@ __device__ __forceinline__ float3 stag_vel(const Grid& g, const float4* __restri
 // counters[0] accumulates clamp events, counters[1] live particles.
 template <bool POW2>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
-                                                const float4* __restrict__ vel,
+                                                const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters) {
     unsigned clamps = 0, live = 0;
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
@@ -232,7 +232,7 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     const int blk = 256;
     long long b = (np + blk - 1) / blk;
     if (b > 148LL * 64) b = 148LL * 64;
-    const float4* v = reinterpret_cast<const float4*>(vel);
+    const float* v = vel;
     if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
         k_advect<true><<<(unsigned)b, blk, 0, s>>>(g, parts, (int)np, v, counters);
     else

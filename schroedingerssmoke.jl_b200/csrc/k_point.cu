@@ -42,45 +42,58 @@ __global__ void k_isjet(Grid g, uint8_t* __restrict__ out, float c0, float c1, f
     }
 }
 
-// staggered sharp on the handle's velocity (examples/benchmark.jl:61-63)
-__global__ void k_sharp(Grid g, float4* __restrict__ vel) {
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
-        const float4 v = vel[c];
-        vel[c] = make_float4(__fmul_rn(v.x, g.dinv[0]), __fmul_rn(v.y, g.dinv[1]), __fmul_rn(v.z, g.dinv[2]), 0.f);
-    }
+// staggered sharp on the handle's padded velocity planes (examples/benchmark.jl:61-63)
+__global__ void k_sharp(Grid g, float* __restrict__ vel) {
+    const long long NP = g.NP;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < 3 * NP; c += (long long)gridDim.x * blockDim.x)
+        vel[c] = __fmul_rn(vel[c], g.dinv[c / NP]);
 }
 
-// div! (parallel.jl:131-152) from the handle's velocity
-__global__ void k_div(Grid g, const float4* __restrict__ vel, float* __restrict__ f) {
-    const long long N = g.N;
-    const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(c % nx);
-        const long long r = c / nx;
-        const int y = (int)(r % ny), z = (int)(r / ny);
-        const long long cxm = (x == 0) ? c + nx - 1 : c - 1;
-        const long long cym = (y == 0) ? c + (long long)(ny - 1) * nx : c - nx;
-        const long long czm = (z == 0) ? c + (long long)(nz - 1) * nx * ny : c - (long long)nx * ny;
-        const float4 v = vel[c];
-        const float t0 = (v.x - vel[cxm].x) * g.inv_d2[0];
-        const float t1 = (v.y - vel[cym].y) * g.inv_d2[1];
-        const float t2 = (v.z - vel[czm].z) * g.inv_d2[2];
+__device__ __forceinline__ void decode(const Grid& g, long long c, int& x, int& y, int& z) {
+    x = (int)(c % g.n[0]);
+    const long long r = c / g.n[0];
+    y = (int)(r % g.n[1]);
+    z = (int)(r / g.n[1]);
+}
+
+// div! (parallel.jl:131-152) from the velocity planes
+__global__ void k_div(Grid g, const float* __restrict__ vel, float* __restrict__ f) {
+    const float* vx = vel;
+    const float* vy = vel + g.NP;
+    const float* vz = vel + 2 * g.NP;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(g, c, x, y, z);
+        const int xm = (x == 0) ? g.n[0] - 1 : x - 1;
+        const int ym = (y == 0) ? g.n[1] - 1 : y - 1;
+        const int zm = (z == 0) ? g.n[2] - 1 : z - 1;
+        const int p = pcell(g, x, y, z);
+        const float t0 = (vx[p] - vx[pcell(g, xm, y, z)]) * g.inv_d2[0];
+        const float t1 = (vy[p] - vy[pcell(g, x, ym, z)]) * g.inv_d2[1];
+        const float t2 = (vz[p] - vz[pcell(g, x, y, zm)]) * g.inv_d2[2];
         f[c] = (t0 + t1) + t2;
     }
 }
 
-__global__ void k_vel_to_aos(Grid g, const float4* __restrict__ vel, float* __restrict__ aos) {
+__global__ void k_vel_to_aos(Grid g, const float* __restrict__ vel, float* __restrict__ aos) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
-        const float4 v = vel[c];
-        aos[3 * c + 0] = v.x;
-        aos[3 * c + 1] = v.y;
-        aos[3 * c + 2] = v.z;
+        int x, y, z;
+        decode(g, c, x, y, z);
+        const int p = pcell(g, x, y, z);
+        aos[3 * c + 0] = vel[p];
+        aos[3 * c + 1] = vel[g.NP + p];
+        aos[3 * c + 2] = vel[2 * g.NP + p];
     }
 }
 
-__global__ void k_vel_from_aos(Grid g, const float* __restrict__ aos, float4* __restrict__ vel) {
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x)
-        vel[c] = make_float4(aos[3 * c + 0], aos[3 * c + 1], aos[3 * c + 2], 0.f);
+__global__ void k_vel_from_aos(Grid g, const float* __restrict__ aos, float* __restrict__ vel) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode(g, c, x, y, z);
+        pstore(g, vel, x, y, z, aos[3 * c + 0]);
+        pstore(g, vel + g.NP, x, y, z, aos[3 * c + 1]);
+        pstore(g, vel + 2 * g.NP, x, y, z, aos[3 * c + 2]);
+    }
 }
 
 __global__ void k_scale_c(float2* __restrict__ a, long long N, float s) {
@@ -105,19 +118,19 @@ cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float le
     return cudaGetLastError();
 }
 cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s) {
-    k_sharp<<<grid_for(g.N, 256), 256, 0, s>>>(g, reinterpret_cast<float4*>(vel));
+    k_sharp<<<grid_for(3 * g.NP, 256), 256, 0, s>>>(g, vel);
     return cudaGetLastError();
 }
 cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s) {
-    k_div<<<grid_for(g.N, 256), 256, 0, s>>>(g, reinterpret_cast<const float4*>(vel), f);
+    k_div<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, f);
     return cudaGetLastError();
 }
 cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s) {
-    k_vel_to_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, reinterpret_cast<const float4*>(vel), aos);
+    k_vel_to_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, aos);
     return cudaGetLastError();
 }
 cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s) {
-    k_vel_from_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, aos, reinterpret_cast<float4*>(vel));
+    k_vel_from_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, aos, vel);
     return cudaGetLastError();
 }
 

@@ -1,15 +1,16 @@
 // z-marching stencil kernels of the velocity one-form.
 //
-// One CTA owns a 32 x 8 column block of the grid and walks up to ST_SZ
-// consecutive z planes.  The padded 34 x 10 psi tile of the current plane
-// sits in shared memory, the tile of the next plane arrives in registers
-// while the current one is worked on (prefetch), so psi is read from HBM
-// about once and each angle of the one-form is evaluated about once per cell.
+// One CTA (256 threads, two rows each) owns a 32 x 16 column block of the
+// grid and walks up to 8 consecutive z planes.  The padded 34 x 18 psi tile of
+// the current plane sits in shared memory, the tile of the next plane arrives
+// in registers while the current one is worked on (prefetch), so psi is read
+// from HBM about once and each angle of the one-form is evaluated about once
+// per cell.
 //
 //   ST_DIV  f = div(velocity_one_form(psi, 1))       parallel.jl:100-122, 131-152
 //           with psi optionally restricted in the nozzle on the fly
 //           (restrict_kernel, particles.jl:12-20)
-//   ST_VEL  velocity (vx, vy, vz, 0) per cell = one_form(psi, hbar) [* 1/d]
+//   ST_VEL  padded velocity planes vx | vy | vz = one_form(psi, hbar) [* 1/d]
 //           (parallel.jl:115-122, staggered sharp examples/benchmark.jl:61-63)
 #include "isf_launch.h"
 
@@ -17,14 +18,20 @@ namespace isf {
 
 namespace {
 
-constexpr int BX = 32, BY = 8, SZ = 16;
-constexpr int TW = BX + 2, TH = BY + 2, TILE = TW * TH;  // padded tile
-constexpr int LPT = (TILE + BX * BY - 1) / (BX * BY);    // tile loads per thread
+#ifndef ISF_ST_SZ
+#define ISF_ST_SZ 8
+#endif
+#ifndef ISF_ST_RPT
+#define ISF_ST_RPT 2
+#endif
+constexpr int BX = 32, TY = 8, RPT = ISF_ST_RPT, BY = TY * RPT, SZ = ISF_ST_SZ;  // 256 threads
+constexpr int TW = BX + 2, TH = BY + 2, TILE = TW * TH;        // padded tile
+constexpr int LPT = (TILE + BX * TY - 1) / (BX * TY);           // tile loads per thread
 
 }  // namespace
 
 template <int OP>
-__global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
+__global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     const Grid& g = a.g;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int tid = threadIdx.x, tx = tid & (BX - 1), ty = tid / BX;
@@ -32,8 +39,10 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
     // partial tiles: the padded tile keeps its halo at column W+1 / row H+1
     const int W = min(BX, nx - x0), H = min(BY, ny - y0);
     const int zend = min(z0 + SZ, nz);
-    const bool own = (tx < W) && (ty < H);
-    const int x = x0 + tx, y = y0 + ty;
+    const int x = x0 + tx;
+    bool own[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) own[m] = (tx < W) && (ty + TY * m < H);
 
     __shared__ float4 tile[2][TH][TW];
     __shared__ float vxs[BY][BX + 1];  // v_x at x0-1+c (c = 0..W)
@@ -46,7 +55,7 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
     int toff[LPT], tx_[LPT], ty_[LPT], tsl[LPT];
 #pragma unroll
     for (int k = 0; k < LPT; ++k) {
-        const int e = tid + k * BX * BY;
+        const int e = tid + k * BX * TY;
         const int r = e / TW, c = e - r * TW;
         const int cc = min(c, W + 1), rr = min(r, H + 1);
         int xx = x0 + cc - 1, yy = y0 + rr - 1;
@@ -77,17 +86,27 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
 #pragma unroll
     for (int k = 0; k < LPT; ++k)
         if (tsl[k] >= 0) pre[k] = tile_e(k, z1);
-    float vz_prev = 0.f;
+    float vz_prev[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) vz_prev[m] = 0.f;
     if constexpr (OP == ST_DIV) {
-        float4 pm = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (own) {
-            const int zm = (z0 == 0) ? nz - 1 : z0 - 1;
-            const long long cm = cell(g, x, y, zm);
-            pm = __ldg(&a.psi[cm]);
-            if (a.use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm);
+        // v_z(z0 - 1) needs psi of plane z0 - 1 at the block's own cells
+        float4 pm[RPT];
+        const int zm = (z0 == 0) ? nz - 1 : z0 - 1;
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            pm[m] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (own[m]) {
+                const int y = y0 + ty + TY * m;
+                const long long cm = cell(g, x, y, zm);
+                pm[m] = __ldg(&a.psi[cm]);
+                if (a.use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm[m]);
+            }
         }
         __syncthreads();
-        if (own) vz_prev = pair_angle(pm, tile[0][ty + 1][tx + 1]);
+#pragma unroll
+        for (int m = 0; m < RPT; ++m)
+            if (own[m]) vz_prev[m] = pair_angle(pm[m], tile[0][ty + TY * m + 1][tx + 1]);
     }
 
     for (int z = z0; z < zend; ++z) {
@@ -103,35 +122,51 @@ __global__ void __launch_bounds__(BX* BY) k_stencil(StencilArgs a) {
             for (int k = 0; k < LPT; ++k)
                 if (tsl[k] >= 0) pre[k] = tile_e(k, z2);
         }
-        const float4 c0 = tile[cur][ty + 1][tx + 1];
         if constexpr (OP == ST_DIV) {
-            if (own) {
-                vxs[ty][tx + 1] = pair_angle(c0, tile[cur][ty + 1][tx + 2]);
-                if (tx == 0) vxs[ty][0] = pair_angle(tile[cur][ty + 1][0], c0);
-                vys[ty + 1][tx] = pair_angle(c0, tile[cur][ty + 2][tx + 1]);
-                if (ty == 0) vys[0][tx] = pair_angle(tile[cur][0][tx + 1], c0);
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                const int r = ty + TY * m;
+                if (own[m]) {
+                    const float4 c0 = tile[cur][r + 1][tx + 1];
+                    vxs[r][tx + 1] = pair_angle(c0, tile[cur][r + 1][tx + 2]);
+                    if (tx == 0) vxs[r][0] = pair_angle(tile[cur][r + 1][0], c0);
+                    vys[r + 1][tx] = pair_angle(c0, tile[cur][r + 2][tx + 1]);
+                    if (r == 0) vys[0][tx] = pair_angle(tile[cur][0][tx + 1], c0);
+                }
             }
             __syncthreads();
-            if (own) {
-                const float vz = pair_angle(c0, tile[nxt][ty + 1][tx + 1]);
-                const float t0 = (vxs[ty][tx + 1] - vxs[ty][tx]) * g.inv_d2[0];
-                const float t1 = (vys[ty + 1][tx] - vys[ty][tx]) * g.inv_d2[1];
-                const float t2 = (vz - vz_prev) * g.inv_d2[2];
-                a.out[cell(g, x, y, z)] = (t0 + t1) + t2;
-                vz_prev = vz;
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                const int r = ty + TY * m;
+                if (own[m]) {
+                    const float vz = pair_angle(tile[cur][r + 1][tx + 1], tile[nxt][r + 1][tx + 1]);
+                    const float t0 = (vxs[r][tx + 1] - vxs[r][tx]) * g.inv_d2[0];
+                    const float t1 = (vys[r + 1][tx] - vys[r][tx]) * g.inv_d2[1];
+                    const float t2 = (vz - vz_prev[m]) * g.inv_d2[2];
+                    a.out[cell(g, x, y0 + r, z)] = (t0 + t1) + t2;
+                    vz_prev[m] = vz;
+                }
             }
         } else {
             __syncthreads();
-            if (own) {
-                float ax = pair_angle(c0, tile[cur][ty + 1][tx + 2]) * a.hbar;
-                float ay = pair_angle(c0, tile[cur][ty + 2][tx + 1]) * a.hbar;
-                float az = pair_angle(c0, tile[nxt][ty + 1][tx + 1]) * a.hbar;
-                if (a.sharp) {
-                    ax = __fmul_rn(ax, g.dinv[0]);
-                    ay = __fmul_rn(ay, g.dinv[1]);
-                    az = __fmul_rn(az, g.dinv[2]);
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                const int r = ty + TY * m;
+                if (own[m]) {
+                    const float4 c0 = tile[cur][r + 1][tx + 1];
+                    float ax = pair_angle(c0, tile[cur][r + 1][tx + 2]) * a.hbar;
+                    float ay = pair_angle(c0, tile[cur][r + 2][tx + 1]) * a.hbar;
+                    float az = pair_angle(c0, tile[nxt][r + 1][tx + 1]) * a.hbar;
+                    if (a.sharp) {
+                        ax = __fmul_rn(ax, g.dinv[0]);
+                        ay = __fmul_rn(ay, g.dinv[1]);
+                        az = __fmul_rn(az, g.dinv[2]);
+                    }
+                    const int y = y0 + r;
+                    pstore(g, a.out, x, y, z, ax);
+                    pstore(g, a.out + g.NP, x, y, z, ay);
+                    pstore(g, a.out + 2 * g.NP, x, y, z, az);
                 }
-                reinterpret_cast<float4*>(a.out)[cell(g, x, y, z)] = make_float4(ax, ay, az, 0.f);
             }
         }
         cur = nxt;
@@ -142,9 +177,9 @@ cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
     dim3 grid((unsigned)((a.g.n[0] + BX - 1) / BX), (unsigned)((a.g.n[1] + BY - 1) / BY),
               (unsigned)((a.g.n[2] + SZ - 1) / SZ));
     if (op == ST_DIV)
-        k_stencil<ST_DIV><<<grid, BX * BY, 0, s>>>(a);
+        k_stencil<ST_DIV><<<grid, BX * TY, 0, s>>>(a);
     else if (op == ST_VEL)
-        k_stencil<ST_VEL><<<grid, BX * BY, 0, s>>>(a);
+        k_stencil<ST_VEL><<<grid, BX * TY, 0, s>>>(a);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
