@@ -150,6 +150,22 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
  * Synchronises the handle's stream. */
 ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);
 
+/* ---- allocation-free entry point (no counterpart in the reference) -------
+ * The real part of poisson_solve (the same result as isf_poisson_solve) for
+ * callers that cannot let the library allocate device memory: a host runtime
+ * whose own pool owns all device memory, a hard memory cap, or a loop that
+ * must not allocate after set-up.  It needs no handle and calls no cudaMalloc
+ * / cudaFree: its workspace is a file-scope device array of 262144 complex64
+ * values (2 MiB, held by every GPU that loads libisf until exit), so
+ * round_up(nx/2 + 1, 16) * ny * nz must not exceed 262144 (ISF_ERR_INVALID
+ * otherwise; e.g. 64 x 64 x 64 fits).  Runs on params->stream (NULL: the
+ * legacy default stream) of params->device; f and q are device arrays of N
+ * floats.  All calls share the workspace: calls that overlap on the GPU race,
+ * so serialise them.  The first call on a device looks up the workspace
+ * address; make it before any stream capture.  Errors: isf_static_last_error(). */
+ISF_API int isf_poisson_solve_static(const isf_params* params, const float* f_dev, float* q_dev);
+ISF_API const char* isf_static_last_error(void);
+
 /* ---- tracing (no reference counterpart beyond @time, examples/benchmark.jl:70) */
 
 /* Per-launch-site CUDA-event timing: between start and stop every kernel

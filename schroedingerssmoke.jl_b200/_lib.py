@@ -22,7 +22,8 @@ EXPORTS = (
     "isf_pressure_project", "isf_velocity_one_form", "isf_staggered_sharp", "isf_get_velocity",
     "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
     "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters", "isf_profile_start",
-    "isf_profile_stop", "isf_profile_sites", "isf_profile_get", "isf_launch_count",
+    "isf_profile_stop", "isf_profile_sites", "isf_profile_get", "isf_launch_count", "isf_poisson_solve_static",
+    "isf_static_last_error",
 )
 
 
@@ -110,6 +111,7 @@ def load(path: str | None = None):
         "isf_profile_sites": [vp, C.POINTER(C.c_int32)],
         "isf_profile_get": [vp, i32, C.c_char_p, sz, C.POINTER(C.c_double), C.POINTER(C.c_int64)],
         "isf_launch_count": [vp, C.POINTER(C.c_uint64)],
+        "isf_poisson_solve_static": [C.POINTER(IsfParams), vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -117,6 +119,8 @@ def load(path: str | None = None):
         fn.restype = C.c_int
     L.isf_last_error.argtypes = [vp]
     L.isf_last_error.restype = C.c_char_p
+    L.isf_static_last_error.argtypes = []
+    L.isf_static_last_error.restype = C.c_char_p
     if path is None:
         _lib = L
     return L

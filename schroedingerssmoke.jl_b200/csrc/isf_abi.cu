@@ -11,6 +11,128 @@
 #include "isf_launch.h"
 #include "isf_passes.cuh"
 
+namespace isf {
+
+int half_spectrum_row(int nx) { return ((nx / 2 + 1 + 15) / 16) * 16; }
+
+size_t table_bytes(const int n[3]) {
+    size_t b = 0;
+    for (int a = 0; a < 3; ++a) b += (sizeof(double2) + sizeof(double) + sizeof(float2)) * (size_t)n[a];
+    return b;
+}
+
+// Grid scalars and the host image of the device tables (ISF constructor,
+// parallel.jl:41-63): per-axis Schroedinger phase factors exp(i th_a(k)) with
+// th_a = (-4 pi^2 hbar) (k'/L_a)^2 dt / 2, k' the fftshift'ed frequency;
+// Laplacian symbols (sin(pi k / n_a) / d_a)^2; twiddles exp(-2 pi i k / n_a).
+// Table layout: mtab (double2) | s2 (double) | tw (float2), each axis after axis.
+void fill_grid(const int n[3], const int L[3], float hbar, float dt, Grid& g, std::vector<char>& host) {
+    const double kPi = 3.14159265358979323846264338327950288;
+    std::memset(&g, 0, sizeof(g));
+    for (int a = 0; a < 3; ++a) {
+        g.n[a] = n[a];
+        g.L[a] = (float)L[a];
+        g.d[a] = (float)((double)L[a] / (double)n[a]);  // parallel.jl:46
+        g.inv_d2[a] = 1.0f / (g.d[a] * g.d[a]);          // parallel.jl:150
+        g.dinv[a] = 1.0f / g.d[a];                        // benchmark.jl:62
+        int ex = 0;
+        g.d_pow2[a] = (std::frexp(g.d[a], &ex) == 0.5f) ? 1 : 0;
+        g.feps[a] = 4.0f * (std::nextafter((float)n[a], 1e30f) - (float)n[a]);
+    }
+    g.N = (long long)n[0] * n[1] * n[2];
+    g.pnx = n[0] + 1;
+    g.pnxy = (n[0] + 1) * (n[1] + 1);
+    g.NP = (long long)g.pnxy * (n[2] + 1);
+    g.hbar = hbar;
+    g.dt = dt;
+    g.invN = 1.0 / (double)g.N;
+
+    size_t mt_bytes = 0, s2_bytes = 0;
+    for (int a = 0; a < 3; ++a) {
+        mt_bytes += sizeof(double2) * n[a];
+        s2_bytes += sizeof(double) * n[a];
+    }
+    host.assign(table_bytes(n), 0);
+    double2* mt = reinterpret_cast<double2*>(host.data());
+    double* s2 = reinterpret_cast<double*>(host.data() + mt_bytes);
+    float2* tw = reinterpret_cast<float2*>(host.data() + mt_bytes + s2_bytes);
+    const double fm = -4.0 * kPi * kPi * (double)hbar;  // f = -4 pi^2 hbar (parallel.jl:49)
+    size_t off = 0;
+    for (int a = 0; a < 3; ++a) {
+        const int na = n[a];
+        for (int k = 0; k < na; ++k) {
+            // fftshift'ed frequency (parallel.jl:58, 62): k' = k for k < n/2, k - n otherwise
+            const double ks = (k < na / 2) ? (double)k : (double)(k - na);
+            const double kk = ks / (double)L[a];
+            const double th = fm * kk * kk * (double)dt / 2.0;
+            mt[off + k] = make_double2(std::cos(th), std::sin(th));
+            const double sn = std::sin(kPi * (double)k / (double)na) / (double)g.d[a];  // parallel.jl:53
+            s2[off + k] = sn * sn;
+            const long double ang = -2.0L * (long double)kPi * (long double)k / (long double)na;
+            tw[off + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        off += na;
+    }
+}
+
+void bind_tables(Grid& g, const char* dev) {
+    size_t mt_bytes = 0, s2_bytes = 0;
+    for (int a = 0; a < 3; ++a) {
+        mt_bytes += sizeof(double2) * g.n[a];
+        s2_bytes += sizeof(double) * g.n[a];
+    }
+    size_t off = 0;
+    for (int a = 0; a < 3; ++a) {
+        g.mtab[a] = reinterpret_cast<const double2*>(dev) + off;
+        g.s2[a] = reinterpret_cast<const double*>(dev + mt_bytes) + off;
+        g.tw[a] = reinterpret_cast<const float2*>(dev + mt_bytes + s2_bytes) + off;
+        off += g.n[a];
+    }
+}
+
+bool valid_grid(const int n[3], std::string& why) {
+    for (int a = 0; a < 3; ++a) {
+        if (!supported_len(n[a])) {
+            why = "grid_res[" + std::to_string(a) + "] = " + std::to_string(n[a]) +
+                  " is not one of 8,12,16,24,32,48,64,96,128,192,256,384,512";
+            return false;
+        }
+    }
+    if (n[0] % 16 != 0) {
+        why = "grid_res[0] must be a multiple of 16";
+        return false;
+    }
+    if (((long long)n[1] * n[2]) % 32 != 0) {
+        why = "grid_res[1]*grid_res[2] must be a multiple of 32";
+        return false;
+    }
+    return true;
+}
+
+bool check_params(const isf_params* p, std::string& why) {
+    if (!p) {
+        why = "null parameters";
+        return false;
+    }
+    if (!valid_grid(p->grid_res, why)) return false;
+    for (int a = 0; a < 3; ++a)
+        if (p->physical_size[a] <= 0) {
+            why = "physical_size must be > 0";
+            return false;
+        }
+    if (!(p->dt > 0.f) || !std::isfinite(p->hbar) || !std::isfinite(p->dt)) {
+        why = "hbar and dt must be finite, dt > 0";
+        return false;
+    }
+    if (p->flags != 0) {
+        why = "flags must be 0";
+        return false;
+    }
+    return true;
+}
+
+}  // namespace isf
+
 using namespace isf;
 
 struct isf_handle {
@@ -136,27 +258,6 @@ struct DeviceGuard {
     DeviceGuard guard_(h->device);                            \
     if (guard_.err != cudaSuccess) return cuda_fail(h, guard_.err, "cudaSetDevice")
 
-const double kPi = 3.14159265358979323846264338327950288;
-
-bool valid_grid(const int n[3], std::string& why) {
-    for (int a = 0; a < 3; ++a) {
-        if (!supported_len(n[a])) {
-            why = "grid_res[" + std::to_string(a) + "] = " + std::to_string(n[a]) +
-                  " is not one of 8,12,16,24,32,48,64,96,128,192,256,384,512";
-            return false;
-        }
-    }
-    if (n[0] % 16 != 0) {
-        why = "grid_res[0] must be a multiple of 16";
-        return false;
-    }
-    if (((long long)n[1] * n[2]) % 32 != 0) {
-        why = "grid_res[1]*grid_res[2] must be a multiple of 32";
-        return false;
-    }
-    return true;
-}
-
 XArgs xargs(isf_handle* h) {
     XArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -259,12 +360,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     if (!p || !out) return fail(nullptr, ISF_ERR_INVALID, "isf_create: null argument");
     *out = nullptr;
     std::string why;
-    if (!valid_grid(p->grid_res, why)) return fail(nullptr, ISF_ERR_INVALID, "isf_create: " + why);
-    for (int a = 0; a < 3; ++a)
-        if (p->physical_size[a] <= 0) return fail(nullptr, ISF_ERR_INVALID, "isf_create: physical_size must be > 0");
-    if (!(p->dt > 0.f) || !std::isfinite(p->hbar) || !std::isfinite(p->dt))
-        return fail(nullptr, ISF_ERR_INVALID, "isf_create: hbar and dt must be finite, dt > 0");
-    if (p->flags != 0) return fail(nullptr, ISF_ERR_INVALID, "isf_create: flags must be 0");
+    if (!check_params(p, why)) return fail(nullptr, ISF_ERR_INVALID, "isf_create: " + why);
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "isf_create: cudaGetDeviceCount");
@@ -278,56 +374,10 @@ int isf_create(const isf_params* p, isf_handle** out) {
         return cuda_fail(nullptr, guard.err, "isf_create: cudaSetDevice");
     }
     Grid& g = h->g;
-    std::memset(&g, 0, sizeof(g));
-    for (int a = 0; a < 3; ++a) {
-        g.n[a] = p->grid_res[a];
-        g.L[a] = (float)p->physical_size[a];
-        g.d[a] = (float)((double)p->physical_size[a] / (double)p->grid_res[a]);  // parallel.jl:46
-        g.inv_d2[a] = 1.0f / (g.d[a] * g.d[a]);                                  // parallel.jl:150
-        g.dinv[a] = 1.0f / g.d[a];                                                // benchmark.jl:62
-        int ex = 0;
-        g.d_pow2[a] = (std::frexp(g.d[a], &ex) == 0.5f) ? 1 : 0;
-        g.feps[a] = 4.0f * (std::nextafter((float)g.n[a], 1e30f) - (float)g.n[a]);
-    }
-    g.N = (long long)g.n[0] * g.n[1] * g.n[2];
-    h->wp = ((g.n[0] / 2 + 1 + 15) / 16) * 16;
-    g.pnx = g.n[0] + 1;
-    g.pnxy = (g.n[0] + 1) * (g.n[1] + 1);
-    g.NP = (long long)g.pnxy * (g.n[2] + 1);
-    g.hbar = p->hbar;
-    g.dt = p->dt;
-    g.invN = 1.0 / (double)g.N;
-
-    // host tables in double
-    size_t tw_bytes = 0, mt_bytes = 0, s2_bytes = 0;
-    for (int a = 0; a < 3; ++a) {
-        tw_bytes += sizeof(float2) * g.n[a];
-        mt_bytes += sizeof(double2) * g.n[a];
-        s2_bytes += sizeof(double) * g.n[a];
-    }
-    const size_t total = mt_bytes + s2_bytes + tw_bytes;
-    std::string host(total, '\0');
-    double2* mt = reinterpret_cast<double2*>(&host[0]);
-    double* s2 = reinterpret_cast<double*>(&host[mt_bytes]);
-    float2* tw = reinterpret_cast<float2*>(&host[mt_bytes + s2_bytes]);
-    const double fm = -4.0 * kPi * kPi * (double)p->hbar;  // f = -4 pi^2 hbar (parallel.jl:49)
-    size_t off = 0;
-    for (int a = 0; a < 3; ++a) {
-        const int n = g.n[a];
-        for (int k = 0; k < n; ++k) {
-            // fftshift'ed frequency (parallel.jl:58, 62): k' = k for k < n/2, k - n otherwise
-            const double ks = (k < n / 2) ? (double)k : (double)(k - n);
-            const double kk = ks / (double)p->physical_size[a];
-            const double th = fm * kk * kk * (double)p->dt / 2.0;
-            mt[off + k] = make_double2(std::cos(th), std::sin(th));
-            const double s = std::sin(kPi * (double)k / (double)n) / (double)g.d[a];  // parallel.jl:53
-            s2[off + k] = s * s;
-            const long double ang = -2.0L * (long double)kPi * (long double)k / (long double)n;
-            tw[off + k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
-        }
-        off += n;
-    }
-
+    std::vector<char> host;
+    fill_grid(p->grid_res, p->physical_size, p->hbar, p->dt, g, host);
+    h->wp = half_spectrum_row(g.n[0]);
+    const size_t total = host.size();
     auto cleanup = [&](int code, const std::string& msg) {
         if (h->F) cudaFree(h->F);
         if (h->f) cudaFree(h->f);
@@ -357,14 +407,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float) * 3 * g.NP);
     if (e == cudaSuccess) e = cudaMemset(h->F, 0, sizeof(float2) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
-    char* base = reinterpret_cast<char*>(h->tables);
-    off = 0;
-    for (int a = 0; a < 3; ++a) {
-        g.mtab[a] = reinterpret_cast<const double2*>(base) + off;
-        g.s2[a] = reinterpret_cast<const double*>(base + mt_bytes) + off;
-        g.tw[a] = reinterpret_cast<const float2*>(base + mt_bytes + s2_bytes) + off;
-        off += g.n[a];
-    }
+    bind_tables(g, reinterpret_cast<const char*>(h->tables));
     *out = h;
     return ISF_OK;
 }

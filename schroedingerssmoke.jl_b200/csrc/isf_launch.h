@@ -3,9 +3,21 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+#include <vector>
+
+#include "../../include/isf.h"
 #include "isf_common.cuh"
 
 namespace isf {
+
+// grid set-up shared by isf_create and the allocation-free entry points (isf_abi.cu)
+bool check_params(const isf_params* p, std::string& why);
+bool valid_grid(const int n[3], std::string& why);
+int half_spectrum_row(int nx);
+size_t table_bytes(const int n[3]);
+void fill_grid(const int n[3], const int L[3], float hbar, float dt, Grid& g, std::vector<char>& host);
+void bind_tables(Grid& g, const char* dev_tables);
 
 struct XArgs;
 struct YZArgs;
