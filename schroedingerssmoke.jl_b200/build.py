@@ -15,7 +15,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CSRC = os.path.join(HERE, "csrc")
+CSRC = os.environ.get("ISF_CSRC") or os.path.join(HERE, "csrc")
 # ISF_CHECK=1 builds the bounds-checking debug variant libisf_check.so
 CHECK = os.environ.get("ISF_CHECK", "0") == "1"
 BUILD = os.environ.get("ISF_BUILD_DIR") or os.path.join(HERE, "_build_check" if CHECK else "_build")

@@ -11,6 +11,11 @@
 #include "isf_launch.h"
 #include "isf_passes.cuh"
 
+// row pitch (floats) of the padded velocity planes is a multiple of this
+#ifndef ISF_VEL_ROW_ALIGN
+#define ISF_VEL_ROW_ALIGN 1
+#endif
+
 namespace isf {
 
 int half_spectrum_row(int nx) { return ((nx / 2 + 1 + 15) / 16) * 16; }
@@ -40,8 +45,8 @@ void fill_grid(const int n[3], const int L[3], float hbar, float dt, Grid& g, st
         g.feps[a] = 4.0f * (std::nextafter((float)n[a], 1e30f) - (float)n[a]);
     }
     g.N = (long long)n[0] * n[1] * n[2];
-    g.pnx = n[0] + 1;
-    g.pnxy = (n[0] + 1) * (n[1] + 1);
+    g.pnx = ((n[0] + 1 + ISF_VEL_ROW_ALIGN - 1) / ISF_VEL_ROW_ALIGN) * ISF_VEL_ROW_ALIGN;
+    g.pnxy = g.pnx * (n[1] + 1);
     g.NP = (long long)g.pnxy * (n[2] + 1);
     g.hbar = hbar;
     g.dt = dt;

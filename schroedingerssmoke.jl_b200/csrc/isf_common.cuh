@@ -5,9 +5,10 @@
 //   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
 //               == NTuple{2,ComplexF32} of src/parallel.jl
 //   velocity    three planes vx | vy | vz (internal to the handle), each
-//               (nx+1) x (ny+1) x (nz+1) with a periodic copy of the x = 0,
-//               y = 0 and z = 0 faces at x = nx, y = ny, z = nz, so the +1
-//               neighbour of any cell is a fixed offset (+1, +pnx, +pnxy)
+//               (nx+1) x (ny+1) x (nz+1) cells (rows padded to 32 floats) with
+//               a periodic copy of the x = 0, y = 0 and z = 0 faces at x = nx,
+//               y = ny, z = nz, so the +1 neighbour of any cell is a fixed
+//               offset (+1, +pnx, +pnxy)
 //   F           float2 per cell: the Poisson spectrum work array
 //   particles   float3 per slot (AoS), dead slot = (-1,-1,-1)
 #pragma once
@@ -30,7 +31,7 @@ struct Grid {
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))
     const double* s2[3];    // (sin(pi k / n_a) / d_a)^2 in double
     double invN;            // 1 / N
-    int pnx, pnxy;          // strides of the padded velocity planes: nx+1, (nx+1)(ny+1)
+    int pnx, pnxy;          // strides of the padded velocity planes: round_up(nx+1, 32), pnx (ny+1)
     long long NP;           // cells of one padded velocity plane
 };
 

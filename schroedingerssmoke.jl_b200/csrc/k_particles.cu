@@ -79,29 +79,6 @@ __device__ __forceinline__ float jl_mod_box(float x, float L) {
     return r;
 }
 
-// Gather of one velocity component.  With -DISF_CHECK (debug builds) every
-// index is validated; a bad one is recorded in chk[0..9] (count, first index,
-// its cell indices, +1 neighbours and strides) and replaced by cell 0.
-__device__ __forceinline__ float vload(const Grid& g, const float* __restrict__ v, int c,
-                                       unsigned long long* chk, const int* ctx) {
-#ifdef ISF_CHECK
-    if (c < 0 || (long long)c >= g.NP) {
-        if (chk) {
-            if (atomicAdd(&chk[0], 1ull) == 0) {
-                chk[1] = (unsigned long long)(unsigned)c;
-                for (int k = 0; k < 8; ++k) chk[2 + k] = (unsigned long long)(unsigned)ctx[k];
-            }
-        }
-        c = 0;
-    }
-#else
-    (void)g;
-    (void)chk;
-    (void)ctx;
-#endif
-    return __ldg(&v[c]);
-}
-
 // floor(fl(p / d)) for p in [0, L]: with d a power of two p * (1/d) is exact;
 // otherwise p * fl(1/d) differs from fl(p / d) by at most 3 ulp(p / d), so
 // when it lies more than eps = 4 ulp(n) from an integer both have the same
@@ -115,52 +92,90 @@ __device__ __forceinline__ int cell_floor(float p, float dinv, float d, float ep
     return (fr > eps && fr < 1.f - eps) ? (int)f1 : __float2int_rd(__fdiv_rn(p, d));
 }
 
-// staggered_velocity (parallel.jl:219-246) on the handle's padded velocity planes.  Interpolation weights are the
-// reference's unnormalised w = p - (i-1) d.  An index that rounds to n (p
-// rounded up to L by mod) is clamped to the last cell and counted.
+// The grid constants the advection needs, copied once into registers (the
+// kernel parameter is otherwise re-read at every RK stage).
+struct AdvConst {
+    float L[3], d[3], dinv[3], feps[3];
+    int nm[3];  // n - 1
+    int pnx, pnxy;
+    const float* __restrict__ vx;
+    const float* __restrict__ vy;
+    const float* __restrict__ vz;
+    long long NP;
+};
+
+__device__ __forceinline__ AdvConst adv_const(const Grid& g, const float* vel) {
+    AdvConst c;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        c.L[a] = g.L[a];
+        c.d[a] = g.d[a];
+        c.dinv[a] = g.dinv[a];
+        c.feps[a] = g.feps[a];
+        c.nm[a] = g.n[a] - 1;
+    }
+    c.pnx = g.pnx;
+    c.pnxy = g.pnxy;
+    c.vx = vel;
+    c.vy = vel + g.NP;
+    c.vz = vel + 2 * g.NP;
+    c.NP = g.NP;
+    return c;
+}
+
+#ifdef ISF_CHECK
+// debug builds: validate a gather index, record the first bad one, read cell 0
+__device__ __forceinline__ int checked(const AdvConst& k, int c, unsigned long long* chk, const int i[3]) {
+    if (c < 0 || (long long)c >= k.NP) {
+        if (chk && atomicAdd(&chk[0], 1ull) == 0) {
+            chk[1] = (unsigned long long)(unsigned)c;
+            for (int a = 0; a < 3; ++a) chk[2 + a] = (unsigned long long)(unsigned)i[a];
+        }
+        return 0;
+    }
+    return c;
+}
+#define ISF_IDX(c) checked(k, (c), chk, i)
+#else
+#define ISF_IDX(c) (c)
+#endif
+
+// staggered_velocity (parallel.jl:219-246) on the handle's padded velocity
+// planes.  Interpolation weights are the reference's unnormalised
+// w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
+// clamped to the last cell and counted.
 template <bool POW2>
-__device__ __forceinline__ float3 stag_vel(const Grid& g, const float* __restrict__ v, float3 pt,
-                                           unsigned& clamps, unsigned long long* chk) {
+__device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigned& clamps, unsigned long long* chk) {
     float P[3] = {pt.x, pt.y, pt.z};
     // mod.(point, ph_size): identity for points inside the box (the common case)
-    const bool inbox = (pt.x >= 0.f && pt.x < g.L[0]) && (pt.y >= 0.f && pt.y < g.L[1]) &&
-                       (pt.z >= 0.f && pt.z < g.L[2]);
+    const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
+                       (pt.z >= 0.f && pt.z < k.L[2]);
     if (!inbox) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], g.L[a]);
+        for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], k.L[a]);
     }
     int i[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const int nm = g.n[a] - 1;
-        int ii = cell_floor<POW2>(P[a], g.dinv[a], g.d[a], g.feps[a]);
-        clamps += (ii > nm);  // mod rounded up to L
-        ii = max(min(ii, nm), 0);
+        int ii = cell_floor<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
+        clamps += (ii > k.nm[a]) ? 1u : 0u;  // mod rounded up to L
+        ii = max(min(ii, k.nm[a]), 0);
         i[a] = ii;
-        w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, g.d[a]));
+        w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, k.d[a]));
     }
+    (void)chk;
     // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell
-    const int sy = g.pnx, sz = g.pnxy;
+    const int sy = k.pnx, sz = k.pnxy;
     const int c000 = i[0] + sy * i[1] + sz * i[2];
     const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
-    const int c011 = c010 + sz, c101 = c100 + sz, c110 = c100 + sy;
-#ifdef ISF_CHECK
-    const int ctx[8] = {i[0], i[1], i[2], c000, c011, c101, sy, sz};
-#else
-    const int* ctx = nullptr;
-#endif
-    // 12 scalar gathers: a warp of cell-sorted particles mostly reads one
-    // address per load, which the L1 serves as one broadcast wavefront
-    const float* __restrict__ vx = v;
-    const float* __restrict__ vy = v + g.NP;
-    const float* __restrict__ vz = v + 2 * g.NP;
-    const float x00 = vload(g, vx, c000, chk, ctx), x10 = vload(g, vx, c010, chk, ctx);
-    const float x01 = vload(g, vx, c001, chk, ctx), x11 = vload(g, vx, c011, chk, ctx);
-    const float y00 = vload(g, vy, c000, chk, ctx), y10 = vload(g, vy, c100, chk, ctx);
-    const float y01 = vload(g, vy, c001, chk, ctx), y11 = vload(g, vy, c101, chk, ctx);
-    const float z00 = vload(g, vz, c000, chk, ctx), z10 = vload(g, vz, c100, chk, ctx);
-    const float z01 = vload(g, vz, c010, chk, ctx), z11 = vload(g, vz, c110, chk, ctx);
+    // 12 scalar gathers (parallel.jl:224-234)
+    const float x00 = __ldg(k.vx + ISF_IDX(c000)), x10 = __ldg(k.vx + ISF_IDX(c010));
+    const float x01 = __ldg(k.vx + ISF_IDX(c001)), x11 = __ldg(k.vx + ISF_IDX(c010 + sz));
+    const float y00 = __ldg(k.vy + ISF_IDX(c000)), y10 = __ldg(k.vy + ISF_IDX(c100));
+    const float y01 = __ldg(k.vy + ISF_IDX(c001)), y11 = __ldg(k.vy + ISF_IDX(c100 + sz));
+    const float z00 = __ldg(k.vz + ISF_IDX(c000)), z10 = __ldg(k.vz + ISF_IDX(c100));
+    const float z01 = __ldg(k.vz + ISF_IDX(c010)), z11 = __ldg(k.vz + ISF_IDX(c100 + sy));
     const float wx = w[0], wy = w[1], wz = w[2];
     float3 u;
     // u_x bilinear in (y, z), u_y in (x, z), u_z in (x, y) (parallel.jl:230-245)
@@ -169,6 +184,7 @@ __device__ __forceinline__ float3 stag_vel(const Grid& g, const float* __restric
     u.z = (1.f - wy) * ((1.f - wx) * z00 + wx * z10) + wy * ((1.f - wx) * z01 + wx * z11);
     return u;
 }
+#undef ISF_IDX
 
 // staggered_advect! (parallel.jl:197-216, 248-261): classical RK4 for every
 // slot inside the open box 0 < p < L, (-1,-1,-1) otherwise.
@@ -177,22 +193,24 @@ template <bool POW2>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters) {
+    const AdvConst kc = adv_const(g, vel);
     unsigned clamps = 0, live = 0;
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
         float3 p = make_float3(parts[3 * k], parts[3 * k + 1], parts[3 * k + 2]);
-        const bool inside = (p.x > 0.f && p.x < g.L[0]) && (p.y > 0.f && p.y < g.L[1]) && (p.z > 0.f && p.z < g.L[2]);
+        const bool inside = (p.x > 0.f && p.x < kc.L[0]) && (p.y > 0.f && p.y < kc.L[1]) &&
+                            (p.z > 0.f && p.z < kc.L[2]);
         if (inside) {
             ++live;
             // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
-            const float3 k1 = stag_vel<POW2>(g, vel, p, clamps, chk);
+            const float3 k1 = stag_vel<POW2>(kc, p, clamps, chk);
             float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-            const float3 k2 = stag_vel<POW2>(g, vel, q, clamps, chk);
+            const float3 k2 = stag_vel<POW2>(kc, q, clamps, chk);
             q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-            const float3 k3 = stag_vel<POW2>(g, vel, q, clamps, chk);
+            const float3 k3 = stag_vel<POW2>(kc, q, clamps, chk);
             q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-            const float3 k4 = stag_vel<POW2>(g, vel, q, clamps, chk);
+            const float3 k4 = stag_vel<POW2>(kc, q, clamps, chk);
             p.x = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
             p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
             p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);

@@ -67,10 +67,20 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
         tsl[k] = (e < TILE) ? e : -1;
     }
     const int nxy = nx * ny;
+    // kernel-parameter fields used in the plane loop, held in registers
+    const float4* __restrict__ psi = a.psi;
+    float* __restrict__ out = a.out;
+    const bool use_jet = a.use_jet != 0;
+    const float id0 = g.inv_d2[0], id1 = g.inv_d2[1], id2 = g.inv_d2[2];
+    const float hb = a.hbar;
+    const bool sharp = a.sharp != 0;
+    const float di0 = g.dinv[0], di1 = g.dinv[1], di2 = g.dinv[2];
+    const int pnx = g.pnx, pnxy = g.pnxy;
+    const int NP = (int)g.NP;
     auto tile_e = [&](int k, int z) -> float4 {
         const int cidx = toff[k] + nxy * z;
-        float4 v = __ldg(&a.psi[cidx]);
-        if (a.use_jet) restrict_cell(g, a.jet, tx_[k], ty_[k], z, cidx, v);
+        float4 v = __ldg(&psi[cidx]);
+        if (use_jet) restrict_cell(g, a.jet, tx_[k], ty_[k], z, cidx, v);
         return v;
     };
     float4* tflat0 = &tile[0][0][0];
@@ -98,9 +108,9 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
             pm[m] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (own[m]) {
                 const int y = y0 + ty + TY * m;
-                const long long cm = cell(g, x, y, zm);
-                pm[m] = __ldg(&a.psi[cm]);
-                if (a.use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm[m]);
+                const int cm = x + nx * y + nxy * zm;
+                pm[m] = __ldg(&psi[cm]);
+                if (use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm[m]);
             }
         }
         __syncthreads();
@@ -140,10 +150,10 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                 const int r = ty + TY * m;
                 if (own[m]) {
                     const float vz = pair_angle(tile[cur][r + 1][tx + 1], tile[nxt][r + 1][tx + 1]);
-                    const float t0 = (vxs[r][tx + 1] - vxs[r][tx]) * g.inv_d2[0];
-                    const float t1 = (vys[r + 1][tx] - vys[r][tx]) * g.inv_d2[1];
-                    const float t2 = (vz - vz_prev[m]) * g.inv_d2[2];
-                    a.out[cell(g, x, y0 + r, z)] = (t0 + t1) + t2;
+                    const float t0 = (vxs[r][tx + 1] - vxs[r][tx]) * id0;
+                    const float t1 = (vys[r + 1][tx] - vys[r][tx]) * id1;
+                    const float t2 = (vz - vz_prev[m]) * id2;
+                    out[x + nx * (y0 + r) + nxy * z] = (t0 + t1) + t2;
                     vz_prev[m] = vz;
                 }
             }
@@ -154,18 +164,24 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                 const int r = ty + TY * m;
                 if (own[m]) {
                     const float4 c0 = tile[cur][r + 1][tx + 1];
-                    float ax = pair_angle(c0, tile[cur][r + 1][tx + 2]) * a.hbar;
-                    float ay = pair_angle(c0, tile[cur][r + 2][tx + 1]) * a.hbar;
-                    float az = pair_angle(c0, tile[nxt][r + 1][tx + 1]) * a.hbar;
-                    if (a.sharp) {
-                        ax = __fmul_rn(ax, g.dinv[0]);
-                        ay = __fmul_rn(ay, g.dinv[1]);
-                        az = __fmul_rn(az, g.dinv[2]);
+                    float ax = pair_angle(c0, tile[cur][r + 1][tx + 2]) * hb;
+                    float ay = pair_angle(c0, tile[cur][r + 2][tx + 1]) * hb;
+                    float az = pair_angle(c0, tile[nxt][r + 1][tx + 1]) * hb;
+                    if (sharp) {
+                        ax = __fmul_rn(ax, di0);
+                        ay = __fmul_rn(ay, di1);
+                        az = __fmul_rn(az, di2);
                     }
                     const int y = y0 + r;
-                    pstore(g, a.out, x, y, z, ax);
-                    pstore(g, a.out + g.NP, x, y, z, ay);
-                    pstore(g, a.out + 2 * g.NP, x, y, z, az);
+                    const int pc = x + pnx * y + pnxy * z;
+                    out[pc] = ax;
+                    out[NP + pc] = ay;
+                    out[2 * NP + pc] = az;
+                    if ((x == 0) | (y == 0) | (z == 0)) {  // periodic copies on the +faces
+                        pstore(g, out, x, y, z, ax);
+                        pstore(g, out + NP, x, y, z, ay);
+                        pstore(g, out + 2 * NP, x, y, z, az);
+                    }
                 }
             }
         }
