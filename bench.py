@@ -80,6 +80,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
     return ap.parse_args()
 
 
@@ -211,6 +212,78 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batched_vs_plain(pkg, cfgs, steps, warmup, local):
+    """The batched ensemble (64 jets on uneven grids, 65 536 particles each,
+    one CUDA graph per step) against the same 64 simulations run one after
+    another through single-simulation handles (isf_step per step, each run
+    synchronised before the next starts).  Both are timed with CUDA events;
+    the sequential runs are bracketed on the legacy default stream, which the
+    handles' blocking streams are ordered with."""
+    import ctypes as C
+    import torch
+    sims, psi0, parts0 = cfgs.ensemble(nsims=64, seed=3, nslots=65536)
+    dev = f"cuda:{local}"
+    b = pkg.ISFBatch(sims, device=local, tune=True)
+    for i in range(len(sims)):
+        b.set_psi(i, torch.from_numpy(psi0[i]).to(dev))
+        b.set_particles(i, torch.from_numpy(parts0[i]).to(dev))
+    b.init_jet(10)
+    b.step(warmup)
+    b.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(b.stream)
+    b.step(steps)
+    e1.record(b.stream)
+    e1.synchronize()
+    t_batch = e0.elapsed_time(e1)
+    ncls, _ = b.classes()
+    tiles = {str(c): b.tiles(c) for c in range(ncls)}
+    b.close()
+
+    # the same simulations, one plain run after another
+    runs = []
+    for i, s in enumerate(sims):
+        h = pkg.ISF(s["physical_size"], s["dims"], s["hbar"], s["dt"], device=local)
+        psi = torch.from_numpy(psi0[i]).to(dev)
+        parts = torch.from_numpy(parts0[i]).to(dev)
+        j = s["jet"]
+        for _ in range(10):
+            pkg.restrict_velocity(h, psi, j["kvec"], None, 0.0, nozzle=(j["cen"], j["len"], j["rad"]),
+                                  phase_mode=j["phase_mode"])
+            pkg.pressure_project(h, psi)
+        dt32 = np.float32(s["dt"])
+        args = []
+        for k in range(1, warmup + steps + 1):
+            t = np.float32(k) * dt32
+            args.append(pkg.step_args(dict(kvec=j["kvec"], omega_t=float(np.float32(j["omega"]) * t), cen=j["cen"],
+                                           len=j["len"], rad=j["rad"], phase_mode=j["phase_mode"],
+                                           emit_mode=j["emit_mode"], emit_count=0, seed=j["seed"], counter=k)))
+        runs.append((h, psi, parts, args))
+    for h, psi, parts, args in runs:
+        for a in args[:warmup]:
+            pkg._lib.check(h.L.isf_step(h.h, C.c_void_p(psi.data_ptr()), C.c_void_p(parts.data_ptr()),
+                                        parts.shape[0], C.byref(a)), h.h)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for h, psi, parts, args in runs:
+        pp, qq, n = C.c_void_p(psi.data_ptr()), C.c_void_p(parts.data_ptr()), parts.shape[0]
+        for a in args[warmup:]:
+            h.L.isf_step(h.h, pp, qq, n, C.byref(a))
+        pkg._lib.check(h.L.isf_sync(h.h), h.h)
+    f1.record()
+    f1.synchronize()
+    t_seq = f0.elapsed_time(f1)
+    for h, *_ in runs:
+        h.close()
+    n = len(sims)
+    return {"workload": "ensemble_64_jets_32^3-96x48x48_65536_particles", "sims": n, "steps": steps,
+            "grids": {str(g): sum(1 for s in sims if tuple(s["dims"]) == g[0]) for g in cfgs.ENSEMBLE_GRIDS},
+            "value": n * steps / (t_batch / 1000.0), "unit": "sim-steps/s",
+            "sequential_value": n * steps / (t_seq / 1000.0), "ratio_vs_sequential": t_seq / t_batch,
+            "ms_per_ensemble_step": t_batch / steps, "classes": ncls, "tiles": tiles}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -334,6 +407,10 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    del isf
+    batched = None
+    if not args.no_batch:
+        batched = batched_vs_plain(pkg, cfgs, min(args.steps, 100), args.warmup, local)
 
     cb = None
     if not args.no_cpu:
@@ -355,6 +432,7 @@ def main():
                           "unit": "GB/s", "frac": step_achieved / peak},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
+        "batched": batched,
     }
     print(json.dumps(line), flush=True)
 

@@ -166,6 +166,78 @@ ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset)
 ISF_API int isf_poisson_solve_static(const isf_params* params, const float* f_dev, float* q_dev);
 ISF_API const char* isf_static_last_error(void);
 
+/* ---- batched ensemble (no single counterpart in the reference: many
+ * independent ISF{...} instances of uneven grid sizes, each driven by the
+ * simloop of examples/benchmark.jl:46-65, stepped together on one GPU) ------
+ *
+ * Simulations with the same grid_res, physical_size, hbar, dt, nslots, jet
+ * flag and emission count share a class; every pass of a step is one launch
+ * per class, and one step of the whole batch is one CUDA graph (replayed per
+ * step) whose class branches run concurrently.  Step k of simulation i is
+ * exactly isf_step on that simulation's psi and particles with
+ *   omega_t    = Float32(omega * Float32(k * dt))   (every product in float),
+ *   emit_start = (k-1) * emit_per_step mod nslots,  counter = k,
+ *   the other isf_step_args fields from its isf_sim_desc (jetmask NULL).
+ * The batch owns all state; psi starts at 0 and every particle slot dead. */
+typedef struct isf_batch isf_batch;
+
+typedef struct isf_sim_desc {
+    int32_t grid_res[3];
+    int32_t physical_size[3];
+    float hbar, dt;
+    int64_t nslots;           /* particle slots (0: no particles) */
+    int32_t jet;              /* 0: plain step (one projection); 1: jet step */
+    int32_t phase_mode;       /* ISF_PHASE_* */
+    float kvec[3];            /* jet_velocity / hbar */
+    float omega;              /* jet frequency: phase k.x - omega t */
+    float nozzle_cen[3];
+    float nozzle_len, nozzle_rad;
+    int32_t emit_mode;        /* ISF_EMIT_* */
+    int64_t emit_per_step;    /* particles emitted per jet step (<= nslots) */
+    uint64_t seed;            /* Philox key of the emission */
+} isf_sim_desc;
+
+/* pass kinds with an autotuned tile (pencil groups per CTA, 1, 2 or 4) */
+enum {
+    ISF_TILE_X_PSI = 0,   /* x passes of psi */
+    ISF_TILE_X_REAL = 1,  /* real-to-complex / complex-to-real x passes of the Poisson solve */
+    ISF_TILE_Y_PSI = 2,   /* y passes of psi */
+    ISF_TILE_Z_PSI = 3,   /* z pass of psi with the Schroedinger phase */
+    ISF_TILE_Y_HALF = 4,  /* y passes of the Poisson half spectrum */
+    ISF_TILE_Z_HALF = 5,  /* z pass of the half spectrum with the inverse Laplacian */
+    ISF_TILE_KINDS = 6
+};
+
+/* Allocate and set up nsims simulations on `device`; tune != 0 runs the tile
+ * autotuner per class (otherwise every tile is 1).  Errors of a failed
+ * create: isf_batch_last_error(NULL). */
+ISF_API int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, int32_t tune, isf_batch** out);
+ISF_API int isf_batch_destroy(isf_batch* b);
+ISF_API const char* isf_batch_last_error(const isf_batch* b);
+/* Copy simulation sim's psi (N float4) or particles (nslots float3) in or out;
+ * the pointer may be host or device memory.  Synchronous. */
+ISF_API int isf_batch_set_psi(isf_batch* b, int32_t sim, const float* psi);
+ISF_API int isf_batch_get_psi(isf_batch* b, int32_t sim, float* psi);
+ISF_API int isf_batch_set_particles(isf_batch* b, int32_t sim, const float* particles);
+ISF_API int isf_batch_get_particles(isf_batch* b, int32_t sim, float* particles);
+/* Device pointers of simulation sim's psi and particles (owned by the batch). */
+ISF_API int isf_batch_state(isf_batch* b, int32_t sim, float** psi, float** particles);
+/* The jet initialisation of examples/benchmark.jl:28-31 for every jet simulation:
+ * iters x (restrict_velocity! at omega t = 0, pressure_project!). */
+ISF_API int isf_batch_init_jet(isf_batch* b, int32_t iters);
+/* nsteps whole time steps of every simulation (asynchronous). */
+ISF_API int isf_batch_step(isf_batch* b, int32_t nsteps);
+/* Set the step counter (the number of the last completed step; 0 after create). */
+ISF_API int isf_batch_set_step(isf_batch* b, int64_t step);
+ISF_API int isf_batch_get_stream(const isf_batch* b, void** stream);
+ISF_API int isf_batch_sync(isf_batch* b);
+/* number of classes, and the class of every simulation (nsims entries, may be NULL) */
+ISF_API int isf_batch_info(const isf_batch* b, int32_t* nclasses, int32_t* sim_class);
+/* the autotuned tile of each pass kind (ISF_TILE_*) of class cls */
+ISF_API int isf_batch_tiles(const isf_batch* b, int32_t cls, int32_t tiles[6]);
+/* [0] clamp events, [1] live particles of simulation sim's advections since the last reset */
+ISF_API int isf_batch_counters(isf_batch* b, int32_t sim, uint64_t out[2], int32_t reset);
+
 /* ---- tracing (no reference counterpart beyond @time, examples/benchmark.jl:70) */
 
 /* Per-launch-site CUDA-event timing: between start and stop every kernel

@@ -24,7 +24,7 @@ from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, PHASE_DOT, PHASE_REFEREN
                    IsfStepArgs, ISFError, check, f3)
 
 __all__ = [
-    "ISF", "ISFError", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
+    "ISF", "ISFBatch", "ISFError", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
     "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
     "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER",
 ]
@@ -284,3 +284,125 @@ def step(isf: ISF, psi: torch.Tensor, particles: torch.Tensor | None = None, jet
     ptr, P = isf._parts(particles)
     a = step_args(jet)
     check(isf.L.isf_step(isf.h, isf._psi(psi), ptr, P, C.byref(a)), isf.h)
+
+
+class ISFBatch:
+    """Many independent simulations stepped together (isf_batch_*): each entry
+    of `sims` is a dict with
+
+        dims, physical_size, hbar, dt        the ISF constructor arguments
+        nslots                               particle slots (default 0)
+        jet                                  None, or a dict with kvec, omega,
+                                             cen, len, rad, phase_mode,
+                                             emit_mode, emit_per_step, seed
+
+    Step k of simulation i equals `step(isf_i, psi_i, particles_i, jet_k)`
+    with omega_t = float32(omega * float32(k * dt)), emit_start =
+    (k-1) * emit_per_step mod nslots and counter = k.  The batch owns psi and
+    the particles; copy them with set_psi / psi / set_particles / particles."""
+
+    def __init__(self, sims, device: int = 0, tune: bool = True):
+        if not torch.cuda.is_available():
+            raise ISFError(_lib.ISF_ERR_CUDA, "no CUDA device: libisf has no CPU path")
+        self.L = _lib.load()
+        n = len(sims)
+        arr = (_lib.IsfSimDesc * n)()
+        self.shapes, self.nslots = [], []
+        for i, s in enumerate(sims):
+            d = arr[i]
+            d.grid_res[:] = [int(x) for x in s["dims"]]
+            d.physical_size[:] = [int(x) for x in s["physical_size"]]
+            d.hbar = float(s["hbar"])
+            d.dt = float(s["dt"])
+            d.nslots = int(s.get("nslots", 0))
+            j = s.get("jet")
+            if j is not None:
+                d.jet = 1
+                d.phase_mode = int(j.get("phase_mode", PHASE_DOT))
+                d.kvec[:] = [float(x) for x in j["kvec"]]
+                d.omega = float(j["omega"])
+                d.nozzle_cen[:] = [float(x) for x in j["cen"]]
+                d.nozzle_len = float(j["len"])
+                d.nozzle_rad = float(j["rad"])
+                d.emit_mode = int(j.get("emit_mode", EMIT_RING))
+                d.emit_per_step = int(j.get("emit_per_step", 0))
+                d.seed = int(j.get("seed", 0))
+            nx, ny, nz = (int(x) for x in s["dims"])
+            self.shapes.append((nz, ny, nx, 4))
+            self.nslots.append(int(d.nslots))
+        b = C.c_void_p()
+        _lib.check_batch(self.L.isf_batch_create(arr, n, int(device), 1 if tune else 0, C.byref(b)))
+        self.b = b
+        self.n = n
+        self.device = torch.device("cuda", int(device))
+        s = C.c_void_p()
+        _lib.check_batch(self.L.isf_batch_get_stream(b, C.byref(s)), b)
+        self.stream = torch.cuda.ExternalStream(s.value, device=self.device)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.isf_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        return _lib.check_batch(rc, self.b)
+
+    def _src(self, t: torch.Tensor, shape):
+        if tuple(t.shape) != tuple(shape) or t.dtype != torch.float32 or not t.is_contiguous():
+            raise ISFError(_lib.ISF_ERR_INVALID, f"expected a contiguous float32 tensor of shape {shape}")
+        if t.is_cuda:
+            torch.cuda.current_stream(t.device).synchronize()
+        return C.c_void_p(t.data_ptr())
+
+    def set_psi(self, i: int, psi: torch.Tensor):
+        self._chk(self.L.isf_batch_set_psi(self.b, int(i), self._src(psi, self.shapes[i])))
+
+    def psi(self, i: int) -> torch.Tensor:
+        out = torch.empty(self.shapes[i], dtype=torch.float32, device=self.device)
+        self._chk(self.L.isf_batch_get_psi(self.b, int(i), C.c_void_p(out.data_ptr())))
+        return out
+
+    def set_particles(self, i: int, parts: torch.Tensor):
+        self._chk(self.L.isf_batch_set_particles(self.b, int(i), self._src(parts, (self.nslots[i], 3))))
+
+    def particles(self, i: int) -> torch.Tensor:
+        out = torch.empty((self.nslots[i], 3), dtype=torch.float32, device=self.device)
+        if self.nslots[i]:
+            self._chk(self.L.isf_batch_get_particles(self.b, int(i), C.c_void_p(out.data_ptr())))
+        return out
+
+    def init_jet(self, iters: int = 10):
+        """examples/benchmark.jl:28-31 for every jet simulation."""
+        self._chk(self.L.isf_batch_init_jet(self.b, int(iters)))
+
+    def step(self, nsteps: int = 1):
+        self._chk(self.L.isf_batch_step(self.b, int(nsteps)))
+
+    def set_step(self, k: int):
+        self._chk(self.L.isf_batch_set_step(self.b, int(k)))
+
+    def sync(self):
+        self._chk(self.L.isf_batch_sync(self.b))
+
+    def classes(self):
+        """(number of classes, class of every simulation)"""
+        nc = C.c_int32()
+        sc = (C.c_int32 * self.n)()
+        self._chk(self.L.isf_batch_info(self.b, C.byref(nc), sc))
+        return nc.value, list(sc)
+
+    def tiles(self, cls: int) -> dict:
+        t = (C.c_int32 * 6)()
+        self._chk(self.L.isf_batch_tiles(self.b, int(cls), t))
+        return dict(zip(_lib.TILE_KINDS, list(t)))
+
+    def counters(self, i: int, reset: bool = False) -> dict:
+        out = (C.c_uint64 * 2)()
+        self._chk(self.L.isf_batch_counters(self.b, int(i), out, 1 if reset else 0))
+        return {"clamps": int(out[0]), "live": int(out[1])}

@@ -23,8 +23,12 @@ EXPORTS = (
     "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
     "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters", "isf_profile_start",
     "isf_profile_stop", "isf_profile_sites", "isf_profile_get", "isf_launch_count", "isf_poisson_solve_static",
-    "isf_static_last_error",
+    "isf_static_last_error", "isf_batch_create", "isf_batch_destroy", "isf_batch_last_error",
+    "isf_batch_set_psi", "isf_batch_get_psi", "isf_batch_set_particles", "isf_batch_get_particles",
+    "isf_batch_state", "isf_batch_init_jet", "isf_batch_step", "isf_batch_set_step", "isf_batch_get_stream",
+    "isf_batch_sync", "isf_batch_info", "isf_batch_tiles", "isf_batch_counters",
 )
+TILE_KINDS = ("x_psi", "x_real", "y_psi", "z_psi", "y_half", "z_half")
 
 
 class ISFError(RuntimeError):
@@ -62,6 +66,26 @@ class IsfStepArgs(C.Structure):
         ("emit_count", C.c_int64),
         ("seed", C.c_uint64),
         ("counter", C.c_uint64),
+    ]
+
+
+class IsfSimDesc(C.Structure):
+    _fields_ = [
+        ("grid_res", C.c_int32 * 3),
+        ("physical_size", C.c_int32 * 3),
+        ("hbar", C.c_float),
+        ("dt", C.c_float),
+        ("nslots", C.c_int64),
+        ("jet", C.c_int32),
+        ("phase_mode", C.c_int32),
+        ("kvec", C.c_float * 3),
+        ("omega", C.c_float),
+        ("nozzle_cen", C.c_float * 3),
+        ("nozzle_len", C.c_float),
+        ("nozzle_rad", C.c_float),
+        ("emit_mode", C.c_int32),
+        ("emit_per_step", C.c_int64),
+        ("seed", C.c_uint64),
     ]
 
 
@@ -112,6 +136,21 @@ def load(path: str | None = None):
         "isf_profile_get": [vp, i32, C.c_char_p, sz, C.POINTER(C.c_double), C.POINTER(C.c_int64)],
         "isf_launch_count": [vp, C.POINTER(C.c_uint64)],
         "isf_poisson_solve_static": [C.POINTER(IsfParams), vp, vp],
+        "isf_batch_create": [C.POINTER(IsfSimDesc), i32, i32, i32, C.POINTER(vp)],
+        "isf_batch_destroy": [vp],
+        "isf_batch_set_psi": [vp, i32, vp],
+        "isf_batch_get_psi": [vp, i32, vp],
+        "isf_batch_set_particles": [vp, i32, vp],
+        "isf_batch_get_particles": [vp, i32, vp],
+        "isf_batch_state": [vp, i32, C.POINTER(vp), C.POINTER(vp)],
+        "isf_batch_init_jet": [vp, i32],
+        "isf_batch_step": [vp, i32],
+        "isf_batch_set_step": [vp, i64],
+        "isf_batch_get_stream": [vp, C.POINTER(vp)],
+        "isf_batch_sync": [vp],
+        "isf_batch_info": [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+        "isf_batch_tiles": [vp, i32, C.POINTER(C.c_int32)],
+        "isf_batch_counters": [vp, i32, C.POINTER(C.c_uint64), i32],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -121,6 +160,8 @@ def load(path: str | None = None):
     L.isf_last_error.restype = C.c_char_p
     L.isf_static_last_error.argtypes = []
     L.isf_static_last_error.restype = C.c_char_p
+    L.isf_batch_last_error.argtypes = [vp]
+    L.isf_batch_last_error.restype = C.c_char_p
     if path is None:
         _lib = L
     return L
@@ -129,6 +170,13 @@ def load(path: str | None = None):
 def check(rc: int, handle=None):
     if rc != ISF_OK:
         msg = load().isf_last_error(handle)
+        raise ISFError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def check_batch(rc: int, batch=None):
+    if rc != ISF_OK:
+        msg = load().isf_batch_last_error(batch)
         raise ISFError(rc, msg.decode() if msg else "")
     return rc
 

@@ -6,7 +6,7 @@ C1  jet, 4x2x2 torus, 64x32x32, hbar 0.1, dt 1/48, 1000 particles/step from
 C2  jet, 4x2x2 torus, 128x64x64, 1M particles seeded in the nozzle (seed 1)
 C3  leapfrogging vortex rings, 10x5x5 torus, 256x128x128, hbar 0.1, dt 1/24,
     4M particles in thin tori around the rings (seed 2), no nozzle
-C4  ensemble of jets on {32^3, 48x32x32, 64x32x32, 96x48x48} with d = 1/16
+C4  ensemble of jets on {32^3, 48x32x32, 64x32x32, 96x48x48} with d = 1/16 (ensemble())
 C5  adjoint jet on the C1 grid (65536 particles)
 
 The reference ships only the jet set-up (examples/benchmark.jl:4-38).  The
@@ -138,3 +138,43 @@ def cell_sort_order(parts: np.ndarray, L, dims) -> np.ndarray:
     ijk = np.clip(np.floor(parts / d).astype(np.int64), 0, np.asarray(dims) - 1)
     key = ijk[:, 0] + dims[0] * (ijk[:, 1] + dims[1] * ijk[:, 2])
     return np.argsort(key, kind="stable")
+
+
+# C4: the ensemble grids, d = 1/16 (physical sizes are integers, as the
+# reference's IntType physical_size requires, src/parallel.jl:12)
+ENSEMBLE_GRIDS = (((32, 32, 32), (2, 2, 2)), ((48, 32, 32), (3, 2, 2)), ((64, 32, 32), (4, 2, 2)),
+                  ((96, 48, 48), (6, 3, 3)))
+
+
+def nozzle_particles(n, cen, length, rad, seed) -> np.ndarray:
+    """n points uniform in the nozzle cylinder (axis x), numpy Philox stream `seed`."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    th = rng.uniform(0, 2 * np.pi, n)
+    r = rad * np.sqrt(rng.uniform(0, 1, n))
+    x = cen[0] + (rng.uniform(0, 1, n) - 0.5) * length
+    return np.ascontiguousarray(np.stack([x, cen[1] + r * np.cos(th), cen[2] + r * np.sin(th)], axis=1))
+
+
+def ensemble(nsims=64, seed=3, nslots=65536, hbar=HBAR, dt=float(np.float32(1 / 48))):
+    """The C4 ensemble: nsims jets on grids drawn uniformly from
+    ENSEMBLE_GRIDS, nozzle speed U[0.5, 1.5] along x, each with nslots
+    particles seeded in its nozzle cylinder at t = 0 and no emission.
+    Returns (batch simulation dicts, psi0 list, particles0 list)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    picks = rng.integers(0, len(ENSEMBLE_GRIDS), nsims)
+    speeds = rng.uniform(0.5, 1.5, nsims)
+    noz = JET_NOZZLE
+    sims, psi0, parts0 = [], [], []
+    h = np.float32(hbar)
+    for i in range(nsims):
+        dims, L = ENSEMBLE_GRIDS[picks[i]]
+        v = np.float32(speeds[i])
+        kvec = (float(v / h), 0.0, 0.0)
+        omega = float(np.float32(v * v / (np.float32(2) * h)))
+        sims.append(dict(dims=dims, physical_size=L, hbar=hbar, dt=dt, nslots=nslots,
+                         jet=dict(kvec=kvec, omega=omega, cen=noz["cen"], len=noz["len"], rad=noz["rad"],
+                                  phase_mode=1, emit_mode=1, emit_per_step=0, seed=seed)))
+        psi0.append(jet_init_psi(dims).astype(np.float32))
+        p = nozzle_particles(nslots, noz["cen"], noz["len"], noz["rad"], seed * 1000 + i)
+        parts0.append(p[cell_sort_order(p, L, dims)].astype(np.float32))
+    return sims, psi0, parts0

@@ -274,6 +274,7 @@ XArgs xargs(isf_handle* h) {
 
 YZArgs yzargs(isf_handle* h, void* data, int axis) {
     YZArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.g = h->g;
     a.data = data;
     a.axis = axis;

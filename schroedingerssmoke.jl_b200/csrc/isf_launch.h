@@ -23,6 +23,8 @@ struct XArgs;
 struct YZArgs;
 
 bool supported_len(int n);
+// a tile of `groups` pencil groups per CTA is available for pencil length n
+bool grouped_tile_ok(int n, int groups);
 
 cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s);
 cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s);
@@ -39,6 +41,12 @@ struct StencilArgs {
     int use_jet;
     float hbar;
     int sharp;
+    // a batch of nsim simulations of this grid (0 or 1: a single one):
+    // simulation s reads psi + s * bs_psi, writes out + s * bs_out and, with
+    // jets != null, restricts with jets[s] instead of jet
+    int nsim;
+    long long bs_psi, bs_out;
+    const JetArgs* jets;
 };
 cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s);
 
@@ -60,9 +68,20 @@ struct EmitArgs {
     uint64_t seed, counter;
     int mode;
 };
+// per-simulation emission of a batch: the arguments and the first ring slot
+struct EmitState {
+    EmitArgs e;
+    long long start;
+};
 cudaError_t launch_emit(float* parts, long long nslots, long long start, long long count, const EmitArgs& e,
                         cudaStream_t s);
+// one launch for nsim simulations: simulation s emits count particles with
+// emits[s] into parts + s * 3 * nslots
+cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, int nsim, const EmitState* emits,
+                              cudaStream_t s);
+// counters: 8 entries per simulation (clamp events, live particles, check records)
+constexpr int kCounterStride = 8;
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel,
-                          unsigned long long* counters, cudaStream_t s);
+                          unsigned long long* counters, cudaStream_t s, int nsim = 1, long long bs_vel = 0);
 
 }  // namespace isf

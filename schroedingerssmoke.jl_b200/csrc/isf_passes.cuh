@@ -12,6 +12,12 @@
 //
 // x pass: lanes run along the row (coalesced 512-byte row segments); y / z
 // passes: lanes run across C consecutive x columns (128-byte segments).
+//
+// Tile shape: a CTA runs G independent groups of C pencils (G = 1, 2 or 4),
+// each with its own [N][C] shared tile, so short pencils (N = 32: 4 threads
+// per pencil) still make CTAs of 128+ threads.  G is chosen per grid by the
+// batch autotuner (isf_batch.cu); single simulations use G = 1.  G changes
+// which pencils share a CTA, never the arithmetic of a pencil.
 #pragma once
 #include <type_traits>
 
@@ -37,6 +43,13 @@ struct XArgs {
     JetArgs jet;
     int use_jet;
     int wp;  // row stride (complex elements) of the half spectrum of real data
+    // a batch of nsim simulations of this grid (blockIdx.y = simulation;
+    // 0 or 1: a single one): element strides between simulations of psi, F
+    // and the real rows, and per-simulation jets (null: jet)
+    int nsim;
+    long long bs_psi, bs_F, bs_r;
+    const JetArgs* jets;
+    int groups;  // pencil groups per CTA (0 or 1: one)
 };
 
 template <int OP>
@@ -47,42 +60,45 @@ struct XTraits {
     static constexpr int S = (OP == X_PSI_FWD || OP == X_C_FWD) ? -1 : +1;
 };
 
-template <int N, int OP>
+template <int N, int OP, int G = 1>
 struct XShape {
     static constexpr int C = XTraits<OP>::C;
     static constexpr int NT = Plan<N>::NT;
-    static constexpr int BLK = C * NT;
-    static constexpr size_t SMEM = (size_t)N * C * sizeof(typename XTraits<OP>::T);
+    static constexpr int BLK = G * C * NT;
+    static constexpr size_t SMEM = (size_t)G * N * C * sizeof(typename XTraits<OP>::T);
 };
 
-template <int N, int OP>
-__global__ void __launch_bounds__(XShape<N, OP>::BLK) k_xpass(XArgs a) {
+template <int N, int OP, int G>
+__global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
     using Tr = XTraits<OP>;
     using T = typename Tr::T;
     constexpr int C = Tr::C;
     constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* sm = reinterpret_cast<T*>(smraw);
-    const int t = threadIdx.x % NT, q = threadIdx.x / NT;
-    const long long row = (long long)blockIdx.x * C + q;
+    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
+    const int t = lt % NT, q = lt / NT;
+    const long long row = ((long long)blockIdx.x * G + grp) * C + q;
     const long long rb = row * N;
+    float4* __restrict__ psi = a.psi + blockIdx.y * a.bs_psi;
+    float2* __restrict__ F = a.F + blockIdx.y * a.bs_F;
     T x[Plan<N>::EMAX];
 
     auto src = [&](int j) -> T {
         if constexpr (Tr::psi_elems) {
-            return a.psi[rb + j];
+            return psi[rb + j];
         } else {
-            return a.F[rb + j];
+            return F[rb + j];
         }
     };
     auto dst = [&](int j, const T& v) {
         if constexpr (OP == X_PSI_FWD || OP == X_PSI_INV) {
-            a.psi[rb + j] = v;
+            psi[rb + j] = v;
         } else if constexpr (OP == X_PSI_INV_NORM) {
-            a.psi[rb + j] = normalize4(v);
+            psi[rb + j] = normalize4(v);
         } else {
             static_assert(OP == X_C_FWD || OP == X_C_INV, "unhandled x-pass op");
-            a.F[rb + j] = v;
+            F[rb + j] = v;
         }
     };
     Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst);
@@ -99,33 +115,36 @@ __global__ void __launch_bounds__(XShape<N, OP>::BLK) k_xpass(XArgs a) {
 // whole 16-column tiles for the y / z passes).
 enum XROp { XR_FWD = 0, XR_INV_GAUGE = 1, XR_INV_REAL = 2 };
 
-template <int N>
+template <int N, int G = 1>
 struct XRShape {
     static constexpr int C = 16;
     static constexpr int NT = Plan<N>::NT;
-    static constexpr int BLK = C * NT;
-    static constexpr size_t SMEM = (size_t)N * C * sizeof(float2);
+    static constexpr int BLK = G * C * NT;
+    static constexpr size_t SMEM = (size_t)G * N * C * sizeof(float2);
 };
 
-template <int N, int OP>
-__global__ void __launch_bounds__(XRShape<N>::BLK) k_xreal(XArgs a) {
+template <int N, int OP, int G>
+__global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
     using T = float2;
     constexpr int C = 16;
     constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* sm = reinterpret_cast<T*>(smraw);
-    const int t = threadIdx.x % NT, q = threadIdx.x / NT;
-    const long long r0 = 2 * ((long long)blockIdx.x * C + q);
+    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
+    const int t = lt % NT, q = lt / NT;
+    const long long r0 = 2 * (((long long)blockIdx.x * G + grp) * C + q);
     const int wp = a.wp;
+    const int sim = blockIdx.y;
+    float2* __restrict__ Fs = a.F + sim * a.bs_F;
     T x[Plan<N>::EMAX];
     if constexpr (OP == XR_FWD) {
-        const float* __restrict__ f0 = a.rin + r0 * N;
+        const float* __restrict__ f0 = a.rin + sim * a.bs_r + r0 * N;
         const float* __restrict__ f1 = f0 + N;
         auto src = [&](int j) -> T { return make_float2(__ldg(&f0[j]), __ldg(&f1[j])); };
         auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
         Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst);
         __syncthreads();
-        float2* __restrict__ A = a.F + r0 * wp;
+        float2* __restrict__ A = Fs + r0 * wp;
         float2* __restrict__ B = A + wp;
 #pragma unroll 1
         for (int k = t; k <= N / 2; k += NT) {
@@ -135,8 +154,12 @@ __global__ void __launch_bounds__(XRShape<N>::BLK) k_xreal(XArgs a) {
             B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
         }
     } else {
-        const float2* __restrict__ A = a.F + r0 * wp;
+        const float2* __restrict__ A = Fs + r0 * wp;
         const float2* __restrict__ B = A + wp;
+        float* __restrict__ rout = a.rout + sim * a.bs_r;
+        float4* __restrict__ psi = a.psi + sim * a.bs_psi;
+        const bool use_jet = a.use_jet != 0;
+        const JetArgs jet = a.jets ? a.jets[sim] : a.jet;
         auto src = [&](int j) -> T {
             if (j <= N / 2) {
                 const float2 u = A[j], v = B[j];
@@ -148,18 +171,18 @@ __global__ void __launch_bounds__(XRShape<N>::BLK) k_xreal(XArgs a) {
         const long long b0 = r0 * N, b1 = b0 + N;
         auto dst = [&](int j, const T& v) {
             if constexpr (OP == XR_INV_REAL) {
-                a.rout[b0 + j] = v.x;
-                a.rout[b1 + j] = v.y;
+                rout[b0 + j] = v.x;
+                rout[b1 + j] = v.y;
             } else {
                 static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
-                float4 p0 = a.psi[b0 + j], p1 = a.psi[b1 + j];
-                if (a.use_jet) {
+                float4 p0 = psi[b0 + j], p1 = psi[b1 + j];
+                if (use_jet) {
                     const int ny = a.g.n[1];
-                    restrict_cell(a.g, a.jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
-                    restrict_cell(a.g, a.jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
+                    restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
+                    restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
                 }
-                a.psi[b0 + j] = gauge4(p0, v.x);
-                a.psi[b1 + j] = gauge4(p1, v.y);
+                psi[b0 + j] = gauge4(p0, v.x);
+                psi[b1 + j] = gauge4(p1, v.y);
             }
         };
         Plan<N>::template run<C, +1, false>(x, t, q, sm, a.g.tw[0], src, dst);
@@ -180,6 +203,9 @@ struct YZArgs {
     int axis;      // 1 (y) or 2 (z)
     int row;       // elements per x row of data (nx, or the padded half-spectrum width)
     int kx_valid;  // columns holding spectrum data; the others are padding
+    int nsim;            // simulations in a batch (blockIdx.z; 0 or 1: one)
+    long long bstride;   // elements between simulations
+    int groups;          // pencil groups per CTA along the other axis (0 or 1: one)
 };
 
 // minimum resident threads per SM the y / z passes are compiled for (caps
@@ -191,12 +217,12 @@ struct YZArgs {
 #define ISF_YZ_SPECTRAL_MIN_THREADS 768
 #endif
 
-template <int N, class T, int OP = 0>
+template <int N, class T, int OP = 0, int G = 1>
 struct YZShape {
     static constexpr int C = 128 / (int)sizeof(T);
     static constexpr int NT = Plan<N>::NT;
-    static constexpr int BLK = C * NT;
-    static constexpr size_t SMEM = (size_t)N * C * sizeof(T);
+    static constexpr int BLK = G * C * NT;
+    static constexpr size_t SMEM = (size_t)G * N * C * sizeof(T);
     static constexpr int MINT = (OP >= 2) ? ISF_YZ_SPECTRAL_MIN_THREADS : ISF_YZ_MIN_THREADS;
     static constexpr int MINB = (MINT / BLK) > 1 ? (MINT / BLK) : 1;
 };
@@ -205,15 +231,17 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-template <int N, class T, int OP>
-__global__ void __launch_bounds__(YZShape<N, T, OP>::BLK, YZShape<N, T, OP>::MINB) k_yzpass(YZArgs a) {
+template <int N, class T, int OP, int G>
+__global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G>::MINB) k_yzpass(YZArgs a) {
     constexpr int C = YZShape<N, T>::C;
+    constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* sm = reinterpret_cast<T*>(smraw);
-    const int q = threadIdx.x % C, t = threadIdx.x / C;
+    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
+    const int q = lt % C, t = lt / C;
     const int rl = a.row, ny = a.g.n[1];
     const int x0 = blockIdx.x * C;
-    const int o = blockIdx.y;
+    const int o = blockIdx.y * G + grp;
     long long stride, base;
     if (a.axis == 1) {
         stride = rl;
@@ -222,7 +250,7 @@ __global__ void __launch_bounds__(YZShape<N, T, OP>::BLK, YZShape<N, T, OP>::MIN
         stride = (long long)rl * ny;
         base = x0 + (long long)o * rl;
     }
-    T* __restrict__ data = reinterpret_cast<T*>(a.data);
+    T* __restrict__ data = reinterpret_cast<T*>(a.data) + blockIdx.z * a.bstride;
     const float2* tw = a.g.tw[a.axis];
     T x[Plan<N>::EMAX];
 

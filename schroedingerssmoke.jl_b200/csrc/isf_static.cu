@@ -124,6 +124,7 @@ int isf_poisson_solve_static(const isf_params* p, const float* f, float* q) {
     xa.rin = f;
     xa.rout = q;
     YZArgs ya;
+    std::memset(&ya, 0, sizeof(ya));
     ya.g = g;
     ya.data = addrs.spectrum;
     ya.row = wp;

@@ -1,9 +1,7 @@
 // Instantiations and launchers of the FFT pass kernels for every supported
-// pencil length (2^a 3^b, 8 <= n <= 512).
-#include <atomic>
-
-#include "isf_launch.h"
-#include "isf_passes.cuh"
+// pencil length (2^a 3^b, 8 <= n <= 512), and the dispatch over the tile
+// shape (pencil groups per CTA) chosen by the caller.
+#include "k_fftpass_impl.cuh"
 
 namespace isf {
 
@@ -15,6 +13,18 @@ bool supported_len(int n) {
         default:
             return false;
     }
+}
+
+// the grouped instantiations live in k_fftpass_g2.cu / k_fftpass_g4.cu
+#define ISF_EXT2(NN) ISF_GROUPED_DECLS(extern, NN, 2)
+#define ISF_EXT4(NN) ISF_GROUPED_DECLS(extern, NN, 4)
+ISF_GROUPED_SIZES(ISF_EXT2)
+ISF_GROUPED_SIZES(ISF_EXT4)
+#undef ISF_EXT2
+#undef ISF_EXT4
+
+bool grouped_tile_ok(int n, int groups) {
+    return groups <= 1 || ((groups == 2 || groups == 4) && n <= kMaxGroupedN && supported_len(n));
 }
 
 #define ISF_SIZE_SWITCH(n, MACRO)                  \
@@ -35,30 +45,14 @@ bool supported_len(int n) {
         default: return cudaErrorInvalidValue;     \
     }
 
-// Kernels needing more than 48 KB of dynamic shared memory must opt in once
-// per device.
-template <class K>
-static cudaError_t ensure_smem(K kernel, size_t smem, std::atomic<unsigned long long>& done) {
-    if (smem <= 48 * 1024) return cudaSuccess;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
-    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
-    return e;
-}
-
 template <int N, int OP>
 static cudaError_t launch_x_n(const XArgs& a, cudaStream_t s) {
-    using Sh = XShape<N, OP>;
-    static std::atomic<unsigned long long> done{0};
-    cudaError_t e = ensure_smem(k_xpass<N, OP>, Sh::SMEM, done);
-    if (e != cudaSuccess) return e;
-    const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    k_xpass<N, OP><<<(unsigned)(rows / Sh::C), Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (N <= kMaxGroupedN && grouped_x_op(OP)) {
+        if (a.groups == 2) return launch_x_ng<N, OP, 2>(a, s);
+        if (a.groups == 4) return launch_x_ng<N, OP, 4>(a, s);
+    }
+    if (a.groups > 1) return cudaErrorInvalidValue;
+    return launch_x_ng<N, OP, 1>(a, s);
 }
 
 template <int OP>
@@ -81,13 +75,12 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
 
 template <int N, int OP>
 static cudaError_t launch_xr_n(const XArgs& a, cudaStream_t s) {
-    using Sh = XRShape<N>;
-    static std::atomic<unsigned long long> done{0};
-    cudaError_t e = ensure_smem(k_xreal<N, OP>, Sh::SMEM, done);
-    if (e != cudaSuccess) return e;
-    const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    k_xreal<N, OP><<<(unsigned)(rows / (2 * Sh::C)), Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    if constexpr (N <= kMaxGroupedN && grouped_xr_op(OP)) {
+        if (a.groups == 2) return launch_xr_ng<N, OP, 2>(a, s);
+        if (a.groups == 4) return launch_xr_ng<N, OP, 4>(a, s);
+    }
+    if (a.groups > 1) return cudaErrorInvalidValue;
+    return launch_xr_ng<N, OP, 1>(a, s);
 }
 
 template <int OP>
@@ -108,14 +101,13 @@ cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s) {
 
 template <int N, class T, int OP>
 static cudaError_t launch_yz_n(const YZArgs& a, cudaStream_t s) {
-    using Sh = YZShape<N, T>;
-    static std::atomic<unsigned long long> done{0};
-    cudaError_t e = ensure_smem(k_yzpass<N, T, OP>, Sh::SMEM, done);
-    if (e != cudaSuccess) return e;
-    const int other = (a.axis == 1) ? a.g.n[2] : a.g.n[1];
-    dim3 grid((unsigned)(a.row / Sh::C), (unsigned)other);
-    k_yzpass<N, T, OP><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    constexpr bool psi = sizeof(T) == sizeof(float4);
+    if constexpr (N <= kMaxGroupedN && grouped_yz_op(OP, psi)) {
+        if (a.groups == 2) return launch_yz_ng<N, T, OP, 2>(a, s);
+        if (a.groups == 4) return launch_yz_ng<N, T, OP, 4>(a, s);
+    }
+    if (a.groups > 1) return cudaErrorInvalidValue;
+    return launch_yz_ng<N, T, OP, 1>(a, s);
 }
 
 template <class T, int OP>

@@ -1,0 +1,10 @@
+// Grouped-tile (G = 2) instantiations of the FFT pass launchers.
+#include "k_fftpass_impl.cuh"
+
+namespace isf {
+
+#define ISF_INST(NN) ISF_GROUPED_DECLS(, NN, 2)
+ISF_GROUPED_SIZES(ISF_INST)
+#undef ISF_INST
+
+}  // namespace isf

@@ -34,9 +34,18 @@ __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0
 // mode 0: the reference ring (0.9 r around (x - 0.1) with +-0.05 jitter,
 //         particles.jl:86-90); 1: uniform in the nozzle disc at x = cen.x;
 //         2: uniform in the nozzle cylinder.
-__global__ void k_emit(float* __restrict__ parts, long long nslots, long long start, long long count, EmitArgs e) {
+// A batch launch (emits != null) handles simulation s = blockIdx.y with
+// emits[s] and its own slots parts + s * 3 * nslots.
+__global__ void k_emit(float* __restrict__ parts, long long nslots, long long start, long long count, EmitArgs e,
+                       const EmitState* __restrict__ emits) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= count) return;
+    if (emits) {
+        const EmitState& st = emits[blockIdx.y];
+        e = st.e;
+        start = st.start;
+        parts += blockIdx.y * 3 * nslots;
+    }
     U4 c = {{(uint32_t)j, (uint32_t)e.counter, (uint32_t)(e.counter >> 32), 0x15F0015Fu}};
     const U4 r = philox4x32_10(c, (uint32_t)e.seed, (uint32_t)(e.seed >> 32));
     const float u0 = u01(r.v[0]), u1 = u01(r.v[1]), u2 = u01(r.v[2]), u3 = u01(r.v[3]);
@@ -189,11 +198,16 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
 // staggered_advect! (parallel.jl:197-216, 248-261): classical RK4 for every
 // slot inside the open box 0 < p < L, (-1,-1,-1) otherwise.
 // counters[0] accumulates clamp events, counters[1] live particles.
+// A batch launch advects simulation s = blockIdx.y: slots parts + s * 3 np,
+// velocity vel + s * bs_vel, counters + s * kCounterStride.
 template <bool POW2>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
-                                                unsigned long long* __restrict__ counters) {
-    const AdvConst kc = adv_const(g, vel);
+                                                unsigned long long* __restrict__ counters, long long bs_vel) {
+    const int sim = blockIdx.y;
+    parts += sim * 3LL * np;
+    if (counters) counters += sim * kCounterStride;
+    const AdvConst kc = adv_const(g, vel + sim * bs_vel);
     unsigned clamps = 0, live = 0;
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
@@ -239,22 +253,32 @@ cudaError_t launch_emit(float* parts, long long nslots, long long start, long lo
                         cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const int blk = 256;
-    k_emit<<<(unsigned)((count + blk - 1) / blk), blk, 0, s>>>(parts, nslots, start, count, e);
+    k_emit<<<(unsigned)((count + blk - 1) / blk), blk, 0, s>>>(parts, nslots, start, count, e, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, int nsim, const EmitState* emits,
+                              cudaStream_t s) {
+    if (count <= 0 || nsim <= 0) return cudaSuccess;
+    if (count > nslots || !emits) return cudaErrorInvalidValue;
+    const int blk = 256;
+    const dim3 grid((unsigned)((count + blk - 1) / blk), (unsigned)nsim);
+    k_emit<<<grid, blk, 0, s>>>(parts, nslots, 0, count, EmitArgs{}, emits);
     return cudaGetLastError();
 }
 
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel, unsigned long long* counters,
-                          cudaStream_t s) {
-    if (np <= 0) return cudaSuccess;
+                          cudaStream_t s, int nsim, long long bs_vel) {
+    if (np <= 0 || nsim <= 0) return cudaSuccess;
     if (np > kMaxParticles) return cudaErrorInvalidValue;
     const int blk = 256;
     long long b = (np + blk - 1) / blk;
     if (b > 148LL * 64) b = 148LL * 64;
-    const float* v = vel;
+    const dim3 grid((unsigned)b, (unsigned)nsim);
     if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
-        k_advect<true><<<(unsigned)b, blk, 0, s>>>(g, parts, (int)np, v, counters);
+        k_advect<true><<<grid, blk, 0, s>>>(g, parts, (int)np, vel, counters, bs_vel);
     else
-        k_advect<false><<<(unsigned)b, blk, 0, s>>>(g, parts, (int)np, v, counters);
+        k_advect<false><<<grid, blk, 0, s>>>(g, parts, (int)np, vel, counters, bs_vel);
     return cudaGetLastError();
 }
 

@@ -35,7 +35,10 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     const Grid& g = a.g;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int tid = threadIdx.x, tx = tid & (BX - 1), ty = tid / BX;
-    const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * SZ;
+    // blockIdx.z = simulation * (z chunks) + z chunk
+    const int zchunks = (nz + SZ - 1) / SZ;
+    const int sim = blockIdx.z / zchunks;
+    const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = (blockIdx.z - sim * zchunks) * SZ;
     // partial tiles: the padded tile keeps its halo at column W+1 / row H+1
     const int W = min(BX, nx - x0), H = min(BY, ny - y0);
     const int zend = min(z0 + SZ, nz);
@@ -68,9 +71,10 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     }
     const int nxy = nx * ny;
     // kernel-parameter fields used in the plane loop, held in registers
-    const float4* __restrict__ psi = a.psi;
-    float* __restrict__ out = a.out;
+    const float4* __restrict__ psi = a.psi + sim * a.bs_psi;
+    float* __restrict__ out = a.out + sim * a.bs_out;
     const bool use_jet = a.use_jet != 0;
+    const JetArgs jet = a.jets ? a.jets[sim] : a.jet;
     const float id0 = g.inv_d2[0], id1 = g.inv_d2[1], id2 = g.inv_d2[2];
     const float hb = a.hbar;
     const bool sharp = a.sharp != 0;
@@ -80,7 +84,7 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     auto tile_e = [&](int k, int z) -> float4 {
         const int cidx = toff[k] + nxy * z;
         float4 v = __ldg(&psi[cidx]);
-        if (use_jet) restrict_cell(g, a.jet, tx_[k], ty_[k], z, cidx, v);
+        if (use_jet) restrict_cell(g, jet, tx_[k], ty_[k], z, cidx, v);
         return v;
     };
     float4* tflat0 = &tile[0][0][0];
@@ -110,7 +114,7 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                 const int y = y0 + ty + TY * m;
                 const int cm = x + nx * y + nxy * zm;
                 pm[m] = __ldg(&psi[cm]);
-                if (use_jet) restrict_cell(g, a.jet, x, y, zm, cm, pm[m]);
+                if (use_jet) restrict_cell(g, jet, x, y, zm, cm, pm[m]);
             }
         }
         __syncthreads();
@@ -190,8 +194,9 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
 }
 
 cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
+    const int nsim = a.nsim > 1 ? a.nsim : 1;
     dim3 grid((unsigned)((a.g.n[0] + BX - 1) / BX), (unsigned)((a.g.n[1] + BY - 1) / BY),
-              (unsigned)((a.g.n[2] + SZ - 1) / SZ));
+              (unsigned)(((a.g.n[2] + SZ - 1) / SZ) * nsim));
     if (op == ST_DIV)
         k_stencil<ST_DIV><<<grid, BX * TY, 0, s>>>(a);
     else if (op == ST_VEL)
