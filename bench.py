@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     return ap.parse_args()
 
 
@@ -284,6 +285,45 @@ def batched_vs_plain(pkg, cfgs, steps, warmup, local):
             "ms_per_ensemble_step": t_batch / steps, "classes": ncls, "tiles": tiles}
 
 
+def adjoint_vs_forward(pkg, cfgs, reps, local):
+    """The particle-loss gradient of the 64x32x32 jet (65 536 particles
+    uniform in the box, 10 initialisation projections, 50 steps, psi
+    checkpointed every 10 steps; isf_adj_gradient) against the forward alone
+    (isf_adj_loss, the same 50 steps).  CUDA events on the handle's stream."""
+    import torch
+    c = cfgs.CONFIGS["C1"]
+    isf = pkg.ISF(c["L"], c["dims"], c["hbar"], c["dt"], device=local)
+    dev = f"cuda:{local}"
+    kvec, omega = cfgs.jet_omega(c["hbar"])
+    noz = cfgs.JET_NOZZLE
+    prob = pkg.adj_problem(50, 10, kvec, omega, (noz["cen"], noz["len"], noz["rad"]), init_iters=10)
+    rng = np.random.Generator(np.random.Philox(4))
+    P = 65536
+    p0 = torch.tensor(rng.uniform(0, 1, (P, 3)) * np.asarray(c["L"]), dtype=torch.float32, device=dev)
+    psi0 = torch.from_numpy(cfgs.jet_init_psi(c["dims"]).astype(np.float32)).to(dev)
+    tgt = p0 + torch.tensor(rng.normal(0, 0.1, (P, 3)), dtype=torch.float32, device=dev)
+    pkg.adj_gradient(isf, prob, psi0, p0, tgt)   # warm-up (allocates the tape)
+    pkg.adj_loss(isf, prob, psi0, p0, tgt)
+    isf.sync()
+    s = isf.stream
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_fwd = timed(lambda: pkg.adj_loss(isf, prob, psi0, p0, tgt))
+    t_grad = timed(lambda: pkg.adj_gradient(isf, prob, psi0, p0, tgt))
+    isf.close()
+    return {"workload": "jet_64x32x32_65536_particles_50_steps_checkpoint_10", "forward_ms": t_fwd,
+            "gradient_ms": t_grad, "ratio_gradient_vs_forward": t_grad / t_fwd,
+            "what": "isf_adj_gradient (forward with checkpoints + segment recompute + reverse) / isf_adj_loss"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -411,6 +451,9 @@ def main():
     batched = None
     if not args.no_batch:
         batched = batched_vs_plain(pkg, cfgs, min(args.steps, 100), args.warmup, local)
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_vs_forward(pkg, cfgs, 3, local)
 
     cb = None
     if not args.no_cpu:
@@ -432,7 +475,7 @@ def main():
                           "unit": "GB/s", "frac": step_achieved / peak},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
-        "batched": batched,
+        "batched": batched, "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 

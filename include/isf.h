@@ -166,6 +166,74 @@ ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset)
 ISF_API int isf_poisson_solve_static(const isf_params* params, const float* f_dev, float* q_dev);
 ISF_API const char* isf_static_last_error(void);
 
+/* ---- adjoint (reverse mode; the reference has no derivatives) -----------
+ * Each isf_adj_* call maps the cotangent of an operator's output to that of
+ * its input at the forward input passed (psi as 4 reals per cell: for every
+ * complex component the cotangent holds dL/dRe, dL/dIm).  Cotangent arrays
+ * are updated in place.  What is differentiated is the reference's own
+ * arithmetic: the angle's branch cut, the unnormalised staggered weights'
+ * jumps at cell faces and the death of particles leaving the box carry no
+ * derivative, so the derivative exists almost everywhere.  The projected
+ * velocity does not change under a phase common to both components of psi
+ * (a gauge), so the jet kvec / omega and such phases have zero gradient
+ * almost everywhere. */
+
+/* schroedinger_flow! transpose (src/parallel.jl:176-187): the flow with conj(mask) */
+ISF_API int isf_adj_schroedinger_flow(isf_handle* h, float* psibar);
+/* normalize_psi (src/parallel.jl:162-165) at psi_in */
+ISF_API int isf_adj_normalize_psi(isf_handle* h, const float* psi_in, float* psibar);
+/* pressure_project! (src/parallel.jl:155-160) at psi_in */
+ISF_API int isf_adj_pressure_project(isf_handle* h, const float* psi_in, float* psibar);
+/* restrict_velocity! (src/particles.jl:12-27) at psi_in; jetbar = cotangents
+ * of (kvec[0], kvec[1], kvec[2], omgterm) */
+ISF_API int isf_adj_restrict_velocity(isf_handle* h, const float* psi_in, float* psibar, const float kvec[3],
+                                      const uint8_t* jetmask_dev, const float cen[3], float len, float rad,
+                                      float omgterm, int32_t phase_mode, double jetbar[4]);
+/* velocity_one_form!(isf, psi, hbar) [+ staggered sharp] (src/parallel.jl:115-122,
+ * examples/benchmark.jl:61-63): consumes the handle's velocity cotangent
+ * (from isf_adj_staggered_advect or isf_adj_set_velocity_bar), adds into
+ * psibar and clears it */
+ISF_API int isf_adj_velocity_one_form(isf_handle* h, const float* psi, float hbar, int32_t sharp, float* psibar);
+/* staggered_advect! (src/parallel.jl:197-261) from `particles` with the
+ * handle's current velocity: particles_bar (after -> before, in place); the
+ * velocity cotangent is added into the handle's */
+ISF_API int isf_adj_staggered_advect(isf_handle* h, const float* particles, float* particles_bar, int64_t np);
+/* the handle's velocity cotangent as / from AoS float3 per cell */
+ISF_API int isf_adj_get_velocity_bar(isf_handle* h, float* vel_aos_dev);
+ISF_API int isf_adj_set_velocity_bar(isf_handle* h, const float* vel_aos_dev);
+/* One whole isf_step, reversed at (psi_in, particles_in): psibar and
+ * particles_bar go from after the step to before it; jetbar = cotangents of
+ * (kvec[0..2], omega_t).  Recomputes the step's forward internally. */
+ISF_API int isf_adj_step(isf_handle* h, const float* psi_in, const float* particles_in, int64_t np,
+                         const isf_step_args* args, float* psibar, float* particles_bar, double jetbar[4]);
+
+/* A jet run whose particle loss is differentiated by isf_adj_gradient:
+ * psi0 -> init_iters x (restrict_velocity! at omega t = 0, pressure_project!)
+ * (examples/benchmark.jl:28-31) -> nsteps jet steps n = 1.. with
+ * omega_t = Float32(omega * Float32(n dt)) and no emission ->
+ * L = sum over particles alive at the end of |x - target|^2. */
+typedef struct isf_adj_problem {
+    int32_t nsteps;
+    int32_t checkpoint_every;  /* psi kept every k steps; the others are recomputed in the reverse pass */
+    int32_t init_iters;
+    int32_t phase_mode;        /* ISF_PHASE_* */
+    float kvec[3];
+    float omega;
+    float nozzle_cen[3];
+    float nozzle_len;
+    float nozzle_rad;
+} isf_adj_problem;
+
+/* L only (the forward of isf_adj_gradient) */
+ISF_API int isf_adj_loss(isf_handle* h, const isf_adj_problem* p, const float* psi0, const float* particles0,
+                         int64_t np, const float* targets, double* loss);
+/* L and its gradient: psibar0 (N float4), particles_bar0 (np float3),
+ * jetbar = dL/d(kvec[0], kvec[1], kvec[2], omega).  Device arrays; psi0 and
+ * particles0 are not modified. */
+ISF_API int isf_adj_gradient(isf_handle* h, const isf_adj_problem* p, const float* psi0, const float* particles0,
+                             int64_t np, const float* targets, double* loss, float* psibar0, float* particles_bar0,
+                             double jetbar[4]);
+
 /* ---- batched ensemble (no single counterpart in the reference: many
  * independent ISF{...} instances of uneven grid sizes, each driven by the
  * simloop of examples/benchmark.jl:46-65, stepped together on one GPU) ------

@@ -388,9 +388,12 @@ struct Orc {
     }
 
     // particles.jl:12-27; phase_mode 0 = reference tuple_dot (sum of k .+ pos),
-    // 1 = k . pos (MatlabPort driver, examples/matlabport/simple.jl:47,107)
-    void restrict_velocity(R* psi, const float kvec[3], const uint8_t* jetmask, const float cen[3], float len,
-                           float rad, float omgterm, int phase_mode) {
+    // 1 = k . pos (MatlabPort driver, examples/matlabport/simple.jl:47,107).
+    // kvec and omgterm arrive in double and are rounded to R: the FP32
+    // restatement sees Float32 values as the reference does, the FP64 oracle
+    // keeps them exact (finite differences in the jet velocity need that).
+    void restrict_velocity(R* psi, const double kvec[3], const uint8_t* jetmask, const float cen[3], float len,
+                           float rad, double omgterm, int phase_mode) {
 #pragma omp parallel for schedule(static)
         for (long z = 0; z < n[2]; ++z)
             for (long y = 0; y < n[1]; ++y)
@@ -644,8 +647,8 @@ void orc_poisson_solve(void* h) { ORC_DISPATCH(h, o.poisson_solve()); }
 void orc_gauge(void* h, void* psi) { ORC_DISPATCH(h, o.gauge((R*)psi)); }
 void orc_pressure_project(void* h, void* psi) { ORC_DISPATCH(h, o.pressure_project((R*)psi)); }
 void orc_staggered_sharp(void* h) { ORC_DISPATCH(h, o.staggered_sharp()); }
-void orc_restrict_velocity(void* h, void* psi, const float* kvec, const uint8_t* jetmask, const float* cen,
-                           float len, float rad, float omgterm, int phase_mode) {
+void orc_restrict_velocity(void* h, void* psi, const double* kvec, const uint8_t* jetmask, const float* cen,
+                           float len, float rad, double omgterm, int phase_mode) {
     ORC_DISPATCH(h, o.restrict_velocity((R*)psi, kvec, jetmask, cen, len, rad, omgterm, phase_mode));
 }
 void orc_isjet(void* h, uint8_t* out, const float* cen, float len, float rad) {
@@ -668,7 +671,7 @@ void orc_staggered_advect(void* h, void* parts, long np, double* margin) {
 
 // One time step in the order of examples/benchmark.jl:46-65.
 // jet == 0: no nozzle (one projection per step).
-void orc_step(void* h, void* psi, void* parts, long np, int jet, const float* kvec, float omega_t,
+void orc_step(void* h, void* psi, void* parts, long np, int jet, const double* kvec, double omega_t,
               const float* cen, float len, float rad, long emit_start, long emit_count, uint64_t seed,
               uint64_t counter, int emit_mode, int phase_mode, double* margin) {
     ORC_DISPATCH(h, {

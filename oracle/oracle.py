@@ -59,6 +59,7 @@ def lib():
         L = C.CDLL(LIB_PATH)
         vp, i32, f32, f64, i64, u64 = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_long, C.c_uint64
         fp = C.POINTER(C.c_float)
+        dp = C.POINTER(C.c_double)
         ip = C.POINTER(C.c_int)
         L.orc_create.restype = vp
         L.orc_create.argtypes = [i32, ip, ip, f32, f32]
@@ -76,18 +77,22 @@ def lib():
         L.orc_clamp_events.restype = i64
         L.orc_clamp_events.argtypes = [vp]
         L.orc_velocity_one_form.argtypes = [vp, vp, f64]
-        L.orc_restrict_velocity.argtypes = [vp, vp, fp, vp, fp, f32, f32, f32, i32]
+        L.orc_restrict_velocity.argtypes = [vp, vp, dp, vp, fp, f32, f32, f64, i32]
         L.orc_isjet.argtypes = [vp, vp, fp, f32, f32]
         L.orc_add_particles.argtypes = [vp, vp, i64, i64, i64, fp, f32, f32, u64, u64, i32]
         L.orc_staggered_advect.argtypes = [vp, vp, i64, vp]
         L.orc_philox.argtypes = [vp, vp, vp]
-        L.orc_step.argtypes = [vp, vp, vp, i64, i32, fp, f32, fp, f32, f32, i64, i64, u64, u64, i32, i32, vp]
+        L.orc_step.argtypes = [vp, vp, vp, i64, i32, dp, f64, fp, f32, f32, i64, i64, u64, u64, i32, i32, vp]
         _lib = L
     return _lib
 
 
 def _f3(v):
     return (C.c_float * 3)(*[float(np.float32(x)) for x in v])
+
+
+def _d3(v):
+    return (C.c_double * 3)(*[float(x) for x in v])
 
 
 def _ptr(a: np.ndarray):
@@ -221,8 +226,8 @@ class Oracle:
 
     def restrict_velocity(self, psi, kvec, omgterm, cen, length, rad, phase_mode=PHASE_DOT, jetmask=None):
         mp = None if jetmask is None else _ptr(np.ascontiguousarray(jetmask, np.uint8))
-        self.L.orc_restrict_velocity(self.h, self._psi(psi), _f3(kvec), mp, _f3(cen), float(length), float(rad),
-                                     float(np.float32(omgterm)), int(phase_mode))
+        self.L.orc_restrict_velocity(self.h, self._psi(psi), _d3(kvec), mp, _f3(cen), float(length), float(rad),
+                                     float(omgterm), int(phase_mode))
         return psi
 
     def add_particles(self, parts, start, count, cen, rad, seed, counter, mode=EMIT_RING, length=0.5):
@@ -248,10 +253,10 @@ class Oracle:
         pp = None if parts is None else _ptr(parts)
         mp = None if margin is None else _ptr(margin)
         if jet is None:
-            self.L.orc_step(self.h, self._psi(psi), pp, np_, 0, _f3((0, 0, 0)), 0.0, _f3((0, 0, 0)), 0.0, 0.0,
+            self.L.orc_step(self.h, self._psi(psi), pp, np_, 0, _d3((0, 0, 0)), 0.0, _f3((0, 0, 0)), 0.0, 0.0,
                             0, 0, 0, 0, 0, 0, mp)
         else:
-            self.L.orc_step(self.h, self._psi(psi), pp, np_, 1, _f3(jet["kvec"]), float(np.float32(jet["omega_t"])),
+            self.L.orc_step(self.h, self._psi(psi), pp, np_, 1, _d3(jet["kvec"]), float(jet["omega_t"]),
                             _f3(jet["cen"]), float(jet["len"]), float(jet["rad"]), int(jet.get("emit_start", 0)),
                             int(jet.get("emit_count", 0)), int(jet.get("seed", 0)), int(jet.get("counter", 0)),
                             int(jet.get("emit_mode", EMIT_RING)), int(jet.get("phase_mode", PHASE_DOT)), mp)

@@ -24,7 +24,7 @@ from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, PHASE_DOT, PHASE_REFEREN
                    IsfStepArgs, ISFError, check, f3)
 
 __all__ = [
-    "ISF", "ISFBatch", "ISFError", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
+    "ISF", "ISFBatch", "ISFError", "ParticleLoss", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
     "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
     "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER",
 ]
@@ -406,3 +406,144 @@ class ISFBatch:
         out = (C.c_uint64 * 2)()
         self._chk(self.L.isf_batch_counters(self.b, int(i), out, 1 if reset else 0))
         return {"clamps": int(out[0]), "live": int(out[1])}
+
+
+# ---------------------------------------------------------------- adjoints
+# The reference has no derivatives; these differentiate its operators
+# (isf_adj_*).  Cotangents are float32 tensors shaped like their primal and
+# are updated in place; psi's cotangent holds (dL/dRe, dL/dIm) per component.
+
+def adj_schroedinger_flow(isf: ISF, psibar: torch.Tensor) -> torch.Tensor:
+    check(isf.L.isf_adj_schroedinger_flow(isf.h, isf._psi(psibar)), isf.h)
+    return psibar
+
+
+def adj_normalize_psi(isf: ISF, psi_in: torch.Tensor, psibar: torch.Tensor) -> torch.Tensor:
+    check(isf.L.isf_adj_normalize_psi(isf.h, isf._psi(psi_in), isf._psi(psibar)), isf.h)
+    return psibar
+
+
+def adj_pressure_project(isf: ISF, psi_in: torch.Tensor, psibar: torch.Tensor) -> torch.Tensor:
+    check(isf.L.isf_adj_pressure_project(isf.h, isf._psi(psi_in), isf._psi(psibar)), isf.h)
+    return psibar
+
+
+def adj_restrict_velocity(isf: ISF, psi_in: torch.Tensor, psibar: torch.Tensor, kvec, omgterm: float = 0.0, *,
+                          nozzle, isjetarr=None, phase_mode: int = PHASE_REFERENCE_SUM):
+    """Returns the cotangents of (kvec[0], kvec[1], kvec[2], omgterm)."""
+    cen, length, rad = nozzle
+    out = (C.c_double * 4)()
+    check(isf.L.isf_adj_restrict_velocity(isf.h, isf._psi(psi_in), isf._psi(psibar), f3(kvec), _ptr(isjetarr),
+                                          f3(cen), float(length), float(rad), float(omgterm), int(phase_mode), out),
+          isf.h)
+    return [float(v) for v in out]
+
+
+def adj_velocity_one_form(isf: ISF, psi: torch.Tensor, psibar: torch.Tensor, hbar: float = 1.0,
+                          sharp: bool = False) -> torch.Tensor:
+    """Consumes the handle's velocity cotangent (see velocity_bar)."""
+    check(isf.L.isf_adj_velocity_one_form(isf.h, isf._psi(psi), float(hbar), 1 if sharp else 0, isf._psi(psibar)),
+          isf.h)
+    return psibar
+
+
+def adj_staggered_advect(isf: ISF, particles: torch.Tensor, particles_bar: torch.Tensor) -> torch.Tensor:
+    ptr, P = isf._parts(particles)
+    bptr, Pb = isf._parts(particles_bar)
+    if P != Pb:
+        raise ISFError(_lib.ISF_ERR_INVALID, "particles and particles_bar differ in length")
+    check(isf.L.isf_adj_staggered_advect(isf.h, ptr, bptr, P), isf.h)
+    return particles_bar
+
+
+def get_velocity_bar(isf: ISF) -> torch.Tensor:
+    out = torch.empty(isf.shape + (3,), dtype=torch.float32, device=isf.device)
+    check(isf.L.isf_adj_get_velocity_bar(isf.h, _ptr(out)), isf.h)
+    return out
+
+
+def set_velocity_bar(isf: ISF, vbar: torch.Tensor) -> None:
+    if vbar.dtype != torch.float32 or tuple(vbar.shape) != isf.shape + (3,):
+        raise ISFError(_lib.ISF_ERR_INVALID, f"velocity cotangent must be float32 {isf.shape + (3,)}")
+    check(isf.L.isf_adj_set_velocity_bar(isf.h, _ptr(vbar)), isf.h)
+
+
+def adj_step(isf: ISF, psi_in: torch.Tensor, particles_in, jet, psibar: torch.Tensor, particles_bar=None):
+    """Reverse of step(isf, psi_in, particles_in, jet); returns the cotangents
+    of (kvec[0..2], omega_t)."""
+    ptr, P = isf._parts(particles_in)
+    bptr, Pb = isf._parts(particles_bar)
+    if P != Pb:
+        raise ISFError(_lib.ISF_ERR_INVALID, "particles and particles_bar differ in length")
+    a = step_args(jet)
+    out = (C.c_double * 4)()
+    check(isf.L.isf_adj_step(isf.h, isf._psi(psi_in), ptr, P, C.byref(a), isf._psi(psibar), bptr, out), isf.h)
+    return [float(v) for v in out]
+
+
+def adj_problem(nsteps, checkpoint_every, kvec, omega, nozzle, init_iters=10, phase_mode=PHASE_DOT):
+    p = _lib.IsfAdjProblem()
+    p.nsteps = int(nsteps)
+    p.checkpoint_every = int(checkpoint_every)
+    p.init_iters = int(init_iters)
+    p.phase_mode = int(phase_mode)
+    p.kvec[:] = [float(x) for x in kvec]
+    p.omega = float(omega)
+    cen, length, rad = nozzle
+    p.nozzle_cen[:] = [float(x) for x in cen]
+    p.nozzle_len = float(length)
+    p.nozzle_rad = float(rad)
+    return p
+
+
+def adj_loss(isf: ISF, problem, psi0, particles0, targets) -> float:
+    ptr, P = isf._parts(particles0)
+    tptr, Pt = isf._parts(targets)
+    if P != Pt:
+        raise ISFError(_lib.ISF_ERR_INVALID, "targets differ in length from the particles")
+    out = C.c_double()
+    check(isf.L.isf_adj_loss(isf.h, C.byref(problem), isf._psi(psi0), ptr, P, tptr, C.byref(out)), isf.h)
+    return float(out.value)
+
+
+def adj_gradient(isf: ISF, problem, psi0, particles0, targets):
+    """(L, dL/dpsi0, dL/dparticles0, dL/d(kvec[0], kvec[1], kvec[2], omega))."""
+    ptr, P = isf._parts(particles0)
+    tptr, Pt = isf._parts(targets)
+    if P != Pt:
+        raise ISFError(_lib.ISF_ERR_INVALID, "targets differ in length from the particles")
+    gpsi = torch.empty_like(psi0)
+    gparts = torch.empty_like(particles0)
+    loss = C.c_double()
+    jb = (C.c_double * 4)()
+    check(isf.L.isf_adj_gradient(isf.h, C.byref(problem), isf._psi(psi0), ptr, P, tptr, C.byref(loss),
+                                 isf._psi(gpsi), _ptr(gparts), jb), isf.h)
+    return float(loss.value), gpsi, gparts, [float(v) for v in jb]
+
+
+class ParticleLoss(torch.autograd.Function):
+    """The jet run's particle loss as a differentiable function of (psi0,
+    kvec, omega) -- the torch counterpart of a ChainRulesCore rrule over
+    isf_adj_gradient.  The forward computes the loss and the gradient in one
+    checkpointed pass; backward scales the stored gradient.
+
+        L = ParticleLoss.apply(psi0, kvec, omega, isf, problem, particles0, targets)
+    """
+
+    @staticmethod
+    def forward(ctx, psi0, kvec, omega, isf, problem, particles0, targets):
+        kv = [float(x) for x in kvec.detach().cpu().tolist()]
+        p = adj_problem(problem.nsteps, problem.checkpoint_every, kv, float(omega), (
+            tuple(problem.nozzle_cen), problem.nozzle_len, problem.nozzle_rad), problem.init_iters, problem.phase_mode)
+        loss, gpsi, _, jb = adj_gradient(isf, p, psi0.detach().contiguous(), particles0, targets)
+        ctx.save_for_backward(gpsi)
+        ctx.jb = jb
+        return torch.tensor(loss, dtype=torch.float64, device=psi0.device)
+
+    @staticmethod
+    def backward(ctx, gout):
+        (gpsi,) = ctx.saved_tensors
+        g = gout.to(torch.float32)
+        gk = torch.tensor(ctx.jb[:3], dtype=torch.float32, device=gpsi.device) * g
+        gw = torch.tensor(ctx.jb[3], dtype=torch.float32, device=gpsi.device) * g
+        return gpsi * g, gk, gw, None, None, None, None

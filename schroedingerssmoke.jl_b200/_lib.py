@@ -27,6 +27,9 @@ EXPORTS = (
     "isf_batch_set_psi", "isf_batch_get_psi", "isf_batch_set_particles", "isf_batch_get_particles",
     "isf_batch_state", "isf_batch_init_jet", "isf_batch_step", "isf_batch_set_step", "isf_batch_get_stream",
     "isf_batch_sync", "isf_batch_info", "isf_batch_tiles", "isf_batch_counters",
+    "isf_adj_schroedinger_flow", "isf_adj_normalize_psi", "isf_adj_pressure_project", "isf_adj_restrict_velocity",
+    "isf_adj_velocity_one_form", "isf_adj_staggered_advect", "isf_adj_get_velocity_bar", "isf_adj_set_velocity_bar",
+    "isf_adj_step", "isf_adj_loss", "isf_adj_gradient",
 )
 TILE_KINDS = ("x_psi", "x_real", "y_psi", "z_psi", "y_half", "z_half")
 
@@ -89,6 +92,20 @@ class IsfSimDesc(C.Structure):
     ]
 
 
+class IsfAdjProblem(C.Structure):
+    _fields_ = [
+        ("nsteps", C.c_int32),
+        ("checkpoint_every", C.c_int32),
+        ("init_iters", C.c_int32),
+        ("phase_mode", C.c_int32),
+        ("kvec", C.c_float * 3),
+        ("omega", C.c_float),
+        ("nozzle_cen", C.c_float * 3),
+        ("nozzle_len", C.c_float),
+        ("nozzle_rad", C.c_float),
+    ]
+
+
 _lib = None
 
 
@@ -104,6 +121,7 @@ def load(path: str | None = None):
     L = C.CDLL(p)
     vp, i32, i64, u64, f32, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_float, C.c_size_t
     fp = C.POINTER(C.c_float)
+    dp = C.POINTER(C.c_double)
     sig = {
         "isf_create": [C.POINTER(IsfParams), C.POINTER(vp)],
         "isf_destroy": [vp],
@@ -151,6 +169,17 @@ def load(path: str | None = None):
         "isf_batch_info": [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
         "isf_batch_tiles": [vp, i32, C.POINTER(C.c_int32)],
         "isf_batch_counters": [vp, i32, C.POINTER(C.c_uint64), i32],
+        "isf_adj_schroedinger_flow": [vp, vp],
+        "isf_adj_normalize_psi": [vp, vp, vp],
+        "isf_adj_pressure_project": [vp, vp, vp],
+        "isf_adj_restrict_velocity": [vp, vp, vp, fp, vp, fp, f32, f32, f32, i32, dp],
+        "isf_adj_velocity_one_form": [vp, vp, f32, i32, vp],
+        "isf_adj_staggered_advect": [vp, vp, vp, i64],
+        "isf_adj_get_velocity_bar": [vp, vp],
+        "isf_adj_set_velocity_bar": [vp, vp],
+        "isf_adj_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs), vp, vp, dp],
+        "isf_adj_loss": [vp, C.POINTER(IsfAdjProblem), vp, vp, i64, vp, dp],
+        "isf_adj_gradient": [vp, C.POINTER(IsfAdjProblem), vp, vp, i64, vp, dp, vp, vp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

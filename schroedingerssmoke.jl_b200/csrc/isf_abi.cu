@@ -8,8 +8,7 @@
 #include <vector>
 
 #include "../../include/isf.h"
-#include "isf_launch.h"
-#include "isf_passes.cuh"
+#include "isf_handle.h"
 
 // row pitch (floats) of the padded velocity planes is a multiple of this
 #ifndef ISF_VEL_ROW_ALIGN
@@ -140,34 +139,8 @@ bool check_params(const isf_params* p, std::string& why) {
 
 using namespace isf;
 
-struct isf_handle {
-    Grid g;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
-    int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
-    float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
-    float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP
-    void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
-    unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
-    unsigned long long launches = 0;         // kernels launched by this handle
-    std::string err;
-    // optional per-launch-site event timing (isf_profile_*)
-    struct Rec {
-        int site;
-        cudaEvent_t a, b;
-    };
-    bool prof_on = false;
-    std::vector<cudaEvent_t> ev_pool;
-    size_t ev_used = 0;
-    std::vector<Rec> recs;
-    std::vector<std::string> site_names;
-    std::vector<double> site_ms;
-    std::vector<long long> site_count;
-};
 
-namespace {
+namespace isf_int {
 
 thread_local std::string g_create_error;
 
@@ -182,10 +155,6 @@ int cuda_fail(isf_handle* h, cudaError_t e, const char* where) {
     return fail(h, ISF_ERR_CUDA, m);
 }
 
-#define ISF_CHECK_HANDLE(h)                                                  \
-    do {                                                                     \
-        if (!(h)) return fail(nullptr, ISF_ERR_INVALID, "null isf handle");  \
-    } while (0)
 
 int prof_site(isf_handle* h, const char* name) {
     for (size_t i = 0; i < h->site_names.size(); ++i)
@@ -222,46 +191,10 @@ void prof_end(isf_handle* h, int slot) {
     if (slot >= 0) cudaEventRecord(h->recs[slot].b, h->stream);
 }
 
-#define ISF_LAUNCH(h, expr, site)                                \
-    do {                                                         \
-        const int ps_ = prof_begin(h, site);                     \
-        cudaError_t e_ = (expr);                                 \
-        ++(h)->launches;                                         \
-        prof_end(h, ps_);                                        \
-        if (e_ != cudaSuccess) return cuda_fail(h, e_, site);    \
-    } while (0)
 
-#define ISF_CUDA(h, expr, where)                      \
-    do {                                              \
-        cudaError_t e_ = (expr);                      \
-        if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
-    } while (0)
 
-// Make the handle's device current for the duration of a call.
-struct DeviceGuard {
-    int prev = -1;
-    cudaError_t err = cudaSuccess;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) err = cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
 
-// psi is read as float4 (16-byte) and complex work arrays as float2 (8-byte)
-#define ISF_ALIGNED(h, ptr, a, name)                                                        \
-    do {                                                                                    \
-        if (((uintptr_t)(ptr)) % (a) != 0)                                                  \
-            return fail(h, ISF_ERR_INVALID, std::string(name) + " must be " #a "-byte aligned"); \
-    } while (0)
 
-#define ISF_ENTER(h)                                          \
-    ISF_CHECK_HANDLE(h);                                      \
-    DeviceGuard guard_(h->device);                            \
-    if (guard_.err != cudaSuccess) return cuda_fail(h, guard_.err, "cudaSetDevice")
 
 XArgs xargs(isf_handle* h) {
     XArgs a;
@@ -358,7 +291,9 @@ JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], f
     return j;
 }
 
-}  // namespace
+}  // namespace isf_int
+
+using namespace isf_int;
 
 extern "C" {
 
@@ -428,6 +363,7 @@ int isf_destroy(isf_handle* h) {
         cudaFree(h->vel);
         cudaFree(h->tables);
         cudaFree(h->counters);
+        adj_free(h);
         if (h->own_stream) cudaStreamDestroy(h->stream);
         for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     }

@@ -1,0 +1,113 @@
+// The ISF handle and the host-side helpers shared by the C ABI files
+// (isf_abi.cu, isf_adj.cu); internal to libisf.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/isf.h"
+#include "isf_launch.h"
+#include "isf_passes.cuh"
+
+struct isf_adj_state;  // adjoint work buffers, allocated on first use (isf_adj.cu)
+
+struct isf_handle {
+    isf::Grid g;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
+    int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
+    float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
+    float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP
+    void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
+    unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
+    unsigned long long launches = 0;         // kernels launched by this handle
+    std::string err;
+    // optional per-launch-site event timing (isf_profile_*)
+    struct Rec {
+        int site;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<Rec> recs;
+    std::vector<std::string> site_names;
+    std::vector<double> site_ms;
+    std::vector<long long> site_count;
+    isf_adj_state* adj = nullptr;
+};
+
+namespace isf_int {
+
+using namespace isf;
+
+int fail(isf_handle* h, int code, const std::string& msg);
+int cuda_fail(isf_handle* h, cudaError_t e, const char* where);
+int prof_begin(isf_handle* h, const char* site);
+void prof_end(isf_handle* h, int slot);
+
+// Make the handle's device current for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+
+// pass arguments of the handle's grid and work arrays
+XArgs xargs(isf_handle* h);
+YZArgs yzargs(isf_handle* h, void* data, int axis);
+YZArgs yzhalf(isf_handle* h, int axis);
+StencilArgs stargs(isf_handle* h, const float* psi, float* out);
+JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], float len, float rad, float omgterm,
+                 int mode);
+
+// kernel sequences of the reference operators (isf_abi.cu)
+int run_schroedinger(isf_handle* h, float* psi, bool norm);
+int run_projection(isf_handle* h, float* psi, const JetArgs* jet);
+int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site);
+
+// releases the adjoint work buffers (isf_adj.cu)
+void adj_free(isf_handle* h);
+
+}  // namespace isf_int
+
+#define ISF_CHECK_HANDLE(h)                                                  \
+    do {                                                                     \
+        if (!(h)) return fail(nullptr, ISF_ERR_INVALID, "null isf handle");  \
+    } while (0)
+
+#define ISF_LAUNCH(h, expr, site)                                \
+    do {                                                         \
+        const int ps_ = prof_begin(h, site);                     \
+        cudaError_t e_ = (expr);                                 \
+        ++(h)->launches;                                         \
+        prof_end(h, ps_);                                        \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, site);    \
+    } while (0)
+
+#define ISF_CUDA(h, expr, where)                      \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
+    } while (0)
+
+// psi is read as float4 (16-byte) and complex work arrays as float2 (8-byte)
+#define ISF_ALIGNED(h, ptr, a, name)                                                        \
+    do {                                                                                    \
+        if (((uintptr_t)(ptr)) % (a) != 0)                                                  \
+            return fail(h, ISF_ERR_INVALID, std::string(name) + " must be " #a "-byte aligned"); \
+    } while (0)
+
+#define ISF_ENTER(h)                                          \
+    ISF_CHECK_HANDLE(h);                                      \
+    DeviceGuard guard_(h->device);                            \
+    if (guard_.err != cudaSuccess) return cuda_fail(h, guard_.err, "cudaSetDevice")

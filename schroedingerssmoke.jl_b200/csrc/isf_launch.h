@@ -84,4 +84,25 @@ constexpr int kCounterStride = 8;
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel,
                           unsigned long long* counters, cudaStream_t s, int nsim = 1, long long bs_vel = 0);
 
+// adjoint kernels (k_adjoint.cu)
+cudaError_t launch_gauge(const Grid& g, const float4* in, const float* q, float4* out, cudaStream_t s);
+cudaError_t launch_normalize_to(const Grid& g, const float4* in, float4* out, cudaStream_t s);
+cudaError_t launch_restrict_to(const Grid& g, const float4* in, float4* out, const JetArgs& j, cudaStream_t s);
+cudaError_t launch_adj_normalize(const Grid& g, const float4* psi_in, float4* bar, cudaStream_t s);
+cudaError_t launch_adj_gauge(const Grid& g, const float4* psi_in, const float* q, float4* bar, float* qbar,
+                             cudaStream_t s);
+cudaError_t launch_adj_oneform_div(const Grid& g, const float4* psi, float4* bar, const float* fbar, cudaStream_t s);
+// folds the padded copies of ubar, then adds the one-form transpose (scale hbar [/ d])
+cudaError_t launch_adj_oneform_vel(const Grid& g, const float4* psi, float4* bar, float* ubar, float hbar, int sharp,
+                                   cudaStream_t s);
+cudaError_t launch_adj_fold(const Grid& g, float* ubar, cudaStream_t s);
+cudaError_t launch_adj_from_aos(const Grid& g, const float* aos, float* ubar, cudaStream_t s);
+// acc[0..2] += cotangent of kvec, acc[3] += cotangent of omega t times wscale
+cudaError_t launch_adj_restrict(const Grid& g, const float4* psi_in, float4* bar, const JetArgs& j, double* acc,
+                                float wscale, cudaStream_t s);
+cudaError_t launch_adj_advect(const Grid& g, const float* parts, float* lam, long long np, const float* vel,
+                              float* ubar, cudaStream_t s);
+cudaError_t launch_loss(const float* x, const float* y, float* lam, long long np, double* loss, cudaStream_t s);
+cudaError_t launch_zero_slots(float* lam, long long nslots, long long start, long long count, cudaStream_t s);
+
 }  // namespace isf

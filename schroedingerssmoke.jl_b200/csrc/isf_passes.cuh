@@ -206,6 +206,7 @@ struct YZArgs {
     int nsim;            // simulations in a batch (blockIdx.z; 0 or 1: one)
     long long bstride;   // elements between simulations
     int groups;          // pencil groups per CTA along the other axis (0 or 1: one)
+    int conj_mask;       // YZ_MASK: multiply by conj(mask) (the adjoint step, dt -> -dt)
 };
 
 // minimum resident threads per SM the y / z passes are compiled for (caps
@@ -274,8 +275,10 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
             cxo.x *= a.g.invN;
             cxo.y *= a.g.invN;
             const double2* __restrict__ mt = a.g.mtab[a.axis];
+            const double msign = a.conj_mask ? -1.0 : 1.0;
             auto mdst = [&](int j, const T& v) {
-                const double2 m = zmul(cxo, __ldg(&mt[j]));
+                double2 m = zmul(cxo, __ldg(&mt[j]));
+                m.y *= msign;
                 sm[sidx<C>(j, q)] = cmul(v, make_float2((float)m.x, (float)m.y));
             };
             Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, mdst);
