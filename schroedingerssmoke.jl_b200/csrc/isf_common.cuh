@@ -55,6 +55,17 @@ __device__ __forceinline__ void pstore(const Grid& g, float* __restrict__ plane,
     }
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization (launch_pdl in isf_launch.h) may start while the kernel
+// before it drains.  pdl_enter lets the next kernel's CTAs be scheduled and
+// then waits until the previous kernel has finished and its writes are
+// visible; every such kernel calls it before its first global memory access.
+// Without the launch attribute both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float4 cadd(float4 a, float4 b) {

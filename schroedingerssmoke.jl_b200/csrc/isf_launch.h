@@ -11,6 +11,25 @@
 
 namespace isf {
 
+// Launch with programmatic stream serialization: the kernel (which must call
+// pdl_enter before touching global memory) may be scheduled while the
+// previous kernel on the stream drains.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // grid set-up shared by isf_create and the allocation-free entry points (isf_abi.cu)
 bool check_params(const isf_params* p, std::string& why);
 bool valid_grid(const int n[3], std::string& why);

@@ -70,6 +70,7 @@ struct XShape {
 
 template <int N, int OP, int G>
 __global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
+    pdl_enter();
     using Tr = XTraits<OP>;
     using T = typename Tr::T;
     constexpr int C = Tr::C;
@@ -125,6 +126,7 @@ struct XRShape {
 
 template <int N, int OP, int G>
 __global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
+    pdl_enter();
     using T = float2;
     constexpr int C = 16;
     constexpr int NT = Plan<N>::NT;
@@ -234,6 +236,7 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 
 template <int N, class T, int OP, int G>
 __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G>::MINB) k_yzpass(YZArgs a) {
+    pdl_enter();
     constexpr int C = YZShape<N, T>::C;
     constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];

@@ -39,8 +39,7 @@ cudaError_t launch_x_ng(const XArgs& a, cudaStream_t s) {
     cudaError_t e = ensure_smem(k_xpass<N, OP, G>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)(rows / (Sh::C * G)), batch_dim(a.nsim));
-    k_xpass<N, OP, G><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_xpass<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 template <int N, int OP, int G>
@@ -52,8 +51,7 @@ cudaError_t launch_xr_ng(const XArgs& a, cudaStream_t s) {
     cudaError_t e = ensure_smem(k_xreal<N, OP, G>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)(rows / (2 * Sh::C * G)), batch_dim(a.nsim));
-    k_xreal<N, OP, G><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_xreal<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 template <int N, class T, int OP, int G>
@@ -65,8 +63,7 @@ cudaError_t launch_yz_ng(const YZArgs& a, cudaStream_t s) {
     cudaError_t e = ensure_smem(k_yzpass<N, T, OP, G>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)(a.row / Sh::C), (unsigned)(other / G), batch_dim(a.nsim));
-    k_yzpass<N, T, OP, G><<<grid, Sh::BLK, Sh::SMEM, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_yzpass<N, T, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 // the grouped instantiations compiled in k_fftpass_g2.cu / k_fftpass_g4.cu:

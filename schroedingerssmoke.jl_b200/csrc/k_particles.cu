@@ -39,6 +39,7 @@ __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0
 // emits[s] and its own slots parts + s * 3 * nslots.
 __global__ void k_emit(float* __restrict__ parts, long long nslots, long long start, long long count, EmitArgs e,
                        const EmitState* __restrict__ emits) {
+    pdl_enter();
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= count) return;
     if (emits) {
@@ -146,6 +147,7 @@ template <bool POW2>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters, long long bs_vel) {
+    pdl_enter();
     const int sim = blockIdx.y;
     parts += sim * 3LL * np;
     if (counters) counters += sim * kCounterStride;
@@ -195,8 +197,8 @@ cudaError_t launch_emit(float* parts, long long nslots, long long start, long lo
                         cudaStream_t s) {
     if (count <= 0) return cudaSuccess;
     const int blk = 256;
-    k_emit<<<(unsigned)((count + blk - 1) / blk), blk, 0, s>>>(parts, nslots, start, count, e, nullptr);
-    return cudaGetLastError();
+    return launch_pdl(k_emit, dim3((unsigned)((count + blk - 1) / blk)), dim3(blk), 0, s, parts, nslots, start, count, e,
+                      (const EmitState*)nullptr);
 }
 
 cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, int nsim, const EmitState* emits,
@@ -205,8 +207,7 @@ cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, i
     if (count > nslots || !emits) return cudaErrorInvalidValue;
     const int blk = 256;
     const dim3 grid((unsigned)((count + blk - 1) / blk), (unsigned)nsim);
-    k_emit<<<grid, blk, 0, s>>>(parts, nslots, 0, count, EmitArgs{}, emits);
-    return cudaGetLastError();
+    return launch_pdl(k_emit, grid, dim3(blk), 0, s, parts, nslots, 0LL, count, EmitArgs{}, emits);
 }
 
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel, unsigned long long* counters,
@@ -218,10 +219,8 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     if (b > 148LL * 64) b = 148LL * 64;
     const dim3 grid((unsigned)b, (unsigned)nsim);
     if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
-        k_advect<true><<<grid, blk, 0, s>>>(g, parts, (int)np, vel, counters, bs_vel);
-    else
-        k_advect<false><<<grid, blk, 0, s>>>(g, parts, (int)np, vel, counters, bs_vel);
-    return cudaGetLastError();
+        return launch_pdl(k_advect<true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
+    return launch_pdl(k_advect<false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
 }
 
 }  // namespace isf

@@ -32,6 +32,7 @@ constexpr int LPT = (TILE + BX * TY - 1) / (BX * TY);           // tile loads pe
 
 template <int OP>
 __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
+    pdl_enter();
     const Grid& g = a.g;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int tid = threadIdx.x, tx = tid & (BX - 1), ty = tid / BX;
@@ -197,13 +198,9 @@ cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
     const int nsim = a.nsim > 1 ? a.nsim : 1;
     dim3 grid((unsigned)((a.g.n[0] + BX - 1) / BX), (unsigned)((a.g.n[1] + BY - 1) / BY),
               (unsigned)(((a.g.n[2] + SZ - 1) / SZ) * nsim));
-    if (op == ST_DIV)
-        k_stencil<ST_DIV><<<grid, BX * TY, 0, s>>>(a);
-    else if (op == ST_VEL)
-        k_stencil<ST_VEL><<<grid, BX * TY, 0, s>>>(a);
-    else
-        return cudaErrorInvalidValue;
-    return cudaGetLastError();
+    if (op == ST_DIV) return launch_pdl(k_stencil<ST_DIV>, grid, dim3(BX * TY), 0, s, a);
+    if (op == ST_VEL) return launch_pdl(k_stencil<ST_VEL>, grid, dim3(BX * TY), 0, s, a);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace isf
