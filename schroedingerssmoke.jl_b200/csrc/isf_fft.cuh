@@ -176,6 +176,24 @@ __device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2
     }
 }
 
+// Like pipeline, but the last stage's outputs stay in x: butterfly
+// i = t + b NT (i < N / R) holds output i + r P at x[b R + r].  That is
+// exactly the input layout of a first stage of radix R with N / R
+// butterflies, so an inverse transform whose radices run in the reverse
+// order can start from these registers without a pass through shared memory.
+template <int N, int NT, int C, int S, class T, int P, int R, int... Rest>
+__device__ __forceinline__ void pipeline_keep(T* x, int t, int q, T* sm, const float2* __restrict__ tw) {
+    butterflies<N, NT, R, P, S>(x, t, tw);
+    if constexpr (sizeof...(Rest) > 0) {
+        scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
+        __syncthreads();
+        constexpr int R2 = First<Rest...>::value;
+        gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
+        __syncthreads();
+        pipeline_keep<N, NT, C, S, T, P * R, Rest...>(x, t, q, sm, tw);
+    }
+}
+
 // --------------------------------------------------------------- radix plans
 constexpr int isf_emax(int N, int NT, std::initializer_list<int> rs) {
     int m = 0;
@@ -187,38 +205,60 @@ constexpr int isf_emax(int N, int NT, std::initializer_list<int> rs) {
     return m;
 }
 
+#define ISF_UNPAREN(...) __VA_ARGS__
+
 // Supported pencil lengths: 2^a 3^b, 8 <= N <= 512.  NT = N / (first radix).
+// FWD lists the radices in stage order, REV the same radices reversed (the
+// inverse of run_spectral).
 template <int N>
 struct Plan;
-#define ISF_PLAN(NN, R0, ...)                                                                               \
+#define ISF_PLAN(NN, R0, FWD, REV)                                                                          \
     template <>                                                                                             \
     struct Plan<NN> {                                                                                       \
         static constexpr int first = R0;                                                                    \
         static constexpr int NT = NN / R0;                                                                  \
-        static constexpr int EMAX = isf_emax(NN, NN / R0, {R0, __VA_ARGS__});                               \
+        static constexpr int EMAX = isf_emax(NN, NN / R0, {ISF_UNPAREN FWD});                              \
         /* SYNC: barrier after the first gather (needed when src reads the tile) */                       \
         template <int C, int S, bool SYNC, class T, class Src, class Dst>                                   \
         static __device__ __forceinline__ void run(T* x, int t, int q, T* sm, const float2* __restrict__ tw, \
                                                    const Src& src, const Dst& dst) {                        \
             gather<NN, NN / R0, R0>(x, t, src);                                                             \
             if constexpr (SYNC) __syncthreads();                                                            \
-            pipeline<NN, NN / R0, C, S, T, Dst, 1, R0, ##__VA_ARGS__>(x, t, q, sm, tw, dst);                \
+            pipeline<NN, NN / R0, C, S, T, Dst, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, dst);                  \
+        }                                                                                                   \
+        /* forward transform, mul(j, v) on every output j in registers, inverse transform */               \
+        template <int C, class T, class Src, class Mul, class Dst>                                          \
+        static __device__ __forceinline__ void run_spectral(T* x, int t, int q, T* sm,                      \
+                                                            const float2* __restrict__ tw, const Src& src,  \
+                                                            const Mul& mul, const Dst& dst) {               \
+            constexpr int NTh = NN / R0;                                                                    \
+            gather<NN, NTh, R0>(x, t, src);                                                                 \
+            pipeline_keep<NN, NTh, C, -1, T, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw);                          \
+            constexpr int RL = First<ISF_UNPAREN REV>::value, PL = NN / RL;                                 \
+            constexpr int NBT = Stage<NN, NTh, RL>::NBT;                                                    \
+            _Pragma("unroll") for (int b = 0; b < NBT; ++b) {                                               \
+                const int i = t + b * NTh;                                                                  \
+                if (PL % NTh == 0 || i < PL) {                                                              \
+                    _Pragma("unroll") for (int r = 0; r < RL; ++r) x[b * RL + r] = mul(i + r * PL, x[b * RL + r]); \
+                }                                                                                           \
+            }                                                                                               \
+            pipeline<NN, NTh, C, +1, T, Dst, 1, ISF_UNPAREN REV>(x, t, q, sm, tw, dst);                     \
         }                                                                                                   \
     };
 
-ISF_PLAN(8, 8)
-ISF_PLAN(12, 4, 3)
-ISF_PLAN(16, 4, 4)
-ISF_PLAN(24, 8, 3)
-ISF_PLAN(32, 8, 4)
-ISF_PLAN(48, 4, 4, 3)
-ISF_PLAN(64, 8, 8)
-ISF_PLAN(96, 8, 4, 3)
-ISF_PLAN(128, 8, 4, 4)
-ISF_PLAN(192, 8, 8, 3)
-ISF_PLAN(256, 8, 8, 4)
-ISF_PLAN(384, 8, 4, 4, 3)
-ISF_PLAN(512, 8, 8, 8)
+ISF_PLAN(8, 8, (8), (8))
+ISF_PLAN(12, 4, (4, 3), (3, 4))
+ISF_PLAN(16, 4, (4, 4), (4, 4))
+ISF_PLAN(24, 8, (8, 3), (3, 8))
+ISF_PLAN(32, 8, (8, 4), (4, 8))
+ISF_PLAN(48, 4, (4, 4, 3), (3, 4, 4))
+ISF_PLAN(64, 8, (8, 8), (8, 8))
+ISF_PLAN(96, 8, (8, 4, 3), (3, 4, 8))
+ISF_PLAN(128, 8, (8, 4, 4), (4, 4, 8))
+ISF_PLAN(192, 8, (8, 8, 3), (3, 8, 8))
+ISF_PLAN(256, 8, (8, 8, 4), (4, 8, 8))
+ISF_PLAN(384, 8, (8, 4, 4, 3), (3, 4, 4, 8))
+ISF_PLAN(512, 8, (8, 8, 8), (8, 8, 8))
 #undef ISF_PLAN
 
 }  // namespace isf

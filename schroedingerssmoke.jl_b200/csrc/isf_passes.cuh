@@ -219,6 +219,11 @@ struct YZArgs {
 #ifndef ISF_YZ_SPECTRAL_MIN_THREADS
 #define ISF_YZ_SPECTRAL_MIN_THREADS 768
 #endif
+// the psi (float4) spectral pass holds twice the data per element: fewer
+// resident threads, more registers (no spills)
+#ifndef ISF_YZ_PSI_SPECTRAL_MIN_THREADS
+#define ISF_YZ_PSI_SPECTRAL_MIN_THREADS 512
+#endif
 
 template <int N, class T, int OP = 0, int G = 1>
 struct YZShape {
@@ -226,7 +231,8 @@ struct YZShape {
     static constexpr int NT = Plan<N>::NT;
     static constexpr int BLK = G * C * NT;
     static constexpr size_t SMEM = (size_t)G * N * C * sizeof(T);
-    static constexpr int MINT = (OP >= 2) ? ISF_YZ_SPECTRAL_MIN_THREADS : ISF_YZ_MIN_THREADS;
+    static constexpr int MINT = (OP < 2) ? ISF_YZ_MIN_THREADS
+                                : (sizeof(T) == 16 ? ISF_YZ_PSI_SPECTRAL_MIN_THREADS : ISF_YZ_SPECTRAL_MIN_THREADS);
     static constexpr int MINB = (MINT / BLK) > 1 ? (MINT / BLK) : 1;
 };
 
@@ -279,12 +285,12 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
             cxo.y *= a.g.invN;
             const double2* __restrict__ mt = a.g.mtab[a.axis];
             const double msign = a.conj_mask ? -1.0 : 1.0;
-            auto mdst = [&](int j, const T& v) {
+            auto mmul = [&](int j, const T& v) -> T {
                 double2 m = zmul(cxo, __ldg(&mt[j]));
                 m.y *= msign;
-                sm[sidx<C>(j, q)] = cmul(v, make_float2((float)m.x, (float)m.y));
+                return cmul(v, make_float2((float)m.x, (float)m.y));
             };
-            Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, mdst);
+            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, mmul, gdst);
         } else {
             static_assert(OP == YZ_FAC, "unhandled y/z op");
             // fac(k)/N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
@@ -294,15 +300,12 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
             const bool zero_line = (kx == 0) && (o == 0);
             const double* __restrict__ s2 = a.g.s2[a.axis];
             const double sc = -0.25 * a.g.invN;
-            auto fdst = [&](int j, const T& v) {
+            auto fmul = [&](int j, const T& v) -> T {
                 const float f = (pad || (zero_line && j == 0)) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2[j])));
-                sm[sidx<C>(j, q)] = cscale(v, f);
+                return cscale(v, f);
             };
-            Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, fdst);
+            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, fmul, gdst);
         }
-        __syncthreads();
-        auto ssrc = [&](int j) -> T { return sm[sidx<C>(j, q)]; };
-        Plan<N>::template run<C, +1, true>(x, t, q, sm, tw, ssrc, gdst);
     }
 }
 
