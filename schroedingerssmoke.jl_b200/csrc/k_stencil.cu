@@ -144,10 +144,17 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                 if (own[m]) {
                     const float4 c0 = tile[cur][r + 1][tx + 1];
                     vxs[r][tx + 1] = pair_angle(c0, tile[cur][r + 1][tx + 2]);
-                    if (tx == 0) vxs[r][0] = pair_angle(tile[cur][r + 1][0], c0);
                     vys[r + 1][tx] = pair_angle(c0, tile[cur][r + 2][tx + 1]);
-                    if (r == 0) vys[0][tx] = pair_angle(tile[cur][0][tx + 1], c0);
                 }
+            }
+            // the tile's halo edges (x0-1 -> x0 per row, y0-1 -> y0 per column),
+            // one per thread of the first two warps rather than one extra
+            // predicated angle in every warp
+            if (tid < BY) {
+                if (tid < H) vxs[tid][0] = pair_angle(tile[cur][tid + 1][0], tile[cur][tid + 1][1]);
+            } else if (tid >= 32 && tid < 32 + BX) {
+                const int c = tid - 32;
+                if (c < W) vys[0][c] = pair_angle(tile[cur][0][c + 1], tile[cur][1][c + 1]);
             }
             __syncthreads();
 #pragma unroll
