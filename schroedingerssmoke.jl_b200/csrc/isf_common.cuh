@@ -5,7 +5,7 @@
 //   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
 //               == NTuple{2,ComplexF32} of src/parallel.jl
 //   velocity    three planes vx | vy | vz (internal to the handle), each
-//               (nx+1) x (ny+1) x (nz+1) cells (rows padded to 32 floats) with
+//               (nx+1) x (ny+1) x (nz+1) cells with
 //               a periodic copy of the x = 0, y = 0 and z = 0 faces at x = nx,
 //               y = ny, z = nz, so the +1 neighbour of any cell is a fixed
 //               offset (+1, +pnx, +pnxy)
@@ -31,7 +31,7 @@ struct Grid {
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))
     const double* s2[3];    // (sin(pi k / n_a) / d_a)^2 in double
     double invN;            // 1 / N
-    int pnx, pnxy;          // strides of the padded velocity planes: round_up(nx+1, 32), pnx (ny+1)
+    int pnx, pnxy;          // strides of the padded velocity planes: nx+1 (rounded up to the row alignment), pnx (ny+1)
     long long NP;           // cells of one padded velocity plane
 };
 
@@ -40,19 +40,27 @@ __host__ __device__ __forceinline__ int pcell(const Grid& g, int x, int y, int z
     return x + g.pnx * y + g.pnxy * z;
 }
 
+// the periodic copies on the +faces of a padded velocity plane of the value
+// at cell index pc (x == 0: cx, ...): seven predicated stores at the fixed
+// offsets ox = nx, oy = ny pnx, oz = nz pnxy
+__device__ __forceinline__ void pcopies(float* __restrict__ plane, int pc, bool cx, bool cy, bool cz, int ox, int oy,
+                                        int oz, float v) {
+    if (cx) plane[pc + ox] = v;
+    if (cy) plane[pc + oy] = v;
+    if (cz) plane[pc + oz] = v;
+    if (cx & cy) plane[pc + ox + oy] = v;
+    if (cx & cz) plane[pc + ox + oz] = v;
+    if (cy & cz) plane[pc + oy + oz] = v;
+    if (cx & cy & cz) plane[pc + ox + oy + oz] = v;
+}
+
 // store v at cell (x, y, z) of a padded velocity plane and at its periodic
 // copies on the +faces (only cells on a low face have copies)
 __device__ __forceinline__ void pstore(const Grid& g, float* __restrict__ plane, int x, int y, int z, float v) {
-    plane[pcell(g, x, y, z)] = v;
-    if ((x == 0) | (y == 0) | (z == 0)) {
-        const int X = (x == 0) ? g.n[0] : x, Y = (y == 0) ? g.n[1] : y, Z = (z == 0) ? g.n[2] : z;
-        // every combination of original / copied coordinate except the original itself
-        for (int m = 1; m < 8; ++m) {
-            const int xx = (m & 1) ? X : x, yy = (m & 2) ? Y : y, zz = (m & 4) ? Z : z;
-            if ((m & 1 && x != 0) || (m & 2 && y != 0) || (m & 4 && z != 0)) continue;
-            plane[pcell(g, xx, yy, zz)] = v;
-        }
-    }
+    const int pc = pcell(g, x, y, z);
+    plane[pc] = v;
+    const bool cx = x == 0, cy = y == 0, cz = z == 0;
+    if (cx | cy | cz) pcopies(plane, pc, cx, cy, cz, g.n[0], g.n[1] * g.pnx, g.n[2] * g.pnxy, v);
 }
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

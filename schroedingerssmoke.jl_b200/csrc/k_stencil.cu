@@ -82,6 +82,7 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     const float di0 = g.dinv[0], di1 = g.dinv[1], di2 = g.dinv[2];
     const int pnx = g.pnx, pnxy = g.pnxy;
     const int NP = (int)g.NP;
+    const int ox = nx, oy = ny * pnx, oz = nz * pnxy;  // +face copy offsets
     auto tile_e = [&](int k, int z) -> float4 {
         const int cidx = toff[k] + nxy * z;
         float4 v = __ldg(&psi[cidx]);
@@ -189,10 +190,11 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                     out[pc] = ax;
                     out[NP + pc] = ay;
                     out[2 * NP + pc] = az;
-                    if ((x == 0) | (y == 0) | (z == 0)) {  // periodic copies on the +faces
-                        pstore(g, out, x, y, z, ax);
-                        pstore(g, out + NP, x, y, z, ay);
-                        pstore(g, out + 2 * NP, x, y, z, az);
+                    const bool cx = x == 0, cy = y == 0, cz = z == 0;
+                    if (cx | cy | cz) {  // periodic copies on the +faces
+                        pcopies(out, pc, cx, cy, cz, ox, oy, oz, ax);
+                        pcopies(out + NP, pc, cx, cy, cz, ox, oy, oz, ay);
+                        pcopies(out + 2 * NP, pc, cx, cy, cz, ox, oy, oz, az);
                     }
                 }
             }
