@@ -180,15 +180,26 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
         parts[3 * k + 2] = p.z;
     }
     if (counters) {
-        // warp-aggregated counters
+        // block-aggregated counters: one atomic per CTA and counter
+        __shared__ unsigned red[2][8];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             clamps += __shfl_down_sync(0xffffffffu, clamps, o);
             live += __shfl_down_sync(0xffffffffu, live, o);
         }
         if ((threadIdx.x & 31) == 0) {
-            if (clamps) atomicAdd(&counters[0], (unsigned long long)clamps);
-            if (live) atomicAdd(&counters[1], (unsigned long long)live);
+            red[0][threadIdx.x >> 5] = clamps;
+            red[1][threadIdx.x >> 5] = live;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long c = 0, l = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                c += red[0][w];
+                l += red[1][w];
+            }
+            if (c) atomicAdd(&counters[0], c);
+            if (l) atomicAdd(&counters[1], l);
         }
     }
 }
@@ -215,8 +226,18 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     if (np <= 0 || nsim <= 0) return cudaSuccess;
     if (np > kMaxParticles) return cudaErrorInvalidValue;
     const int blk = 256;
+    // one resident wave, grid-stride over the slots
+    static int resident = 0;  // CTAs per SM of either instantiation (the same registers)
+    if (resident == 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false>, blk, 0) != cudaSuccess || per < 1)
+            return cudaErrorInvalidValue;
+        resident = sms * per;
+    }
     long long b = (np + blk - 1) / blk;
-    if (b > 148LL * 64) b = 148LL * 64;
+    if (b > resident) b = resident;
     const dim3 grid((unsigned)b, (unsigned)nsim);
     if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
         return launch_pdl(k_advect<true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
