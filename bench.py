@@ -56,6 +56,7 @@ SITE_BYTES_PER_CELL = {
     "projection x fwd": 4 + HALF_SPECTRUM,         # f read, half spectrum write
     "projection y fwd": 2 * HALF_SPECTRUM, "projection z fac": 2 * HALF_SPECTRUM,
     "projection y inv": 2 * HALF_SPECTRUM,         # half spectrum read + write
+    "projection yz planes": 2 * HALF_SPECTRUM,     # k-major half spectrum read + write once
     "projection x inv + gauge": HALF_SPECTRUM + 32,   # half spectrum read, psi read + write
     "step one_form": 28,                           # psi read, velocity write (3 floats)
     "step advect": 12,                             # velocity read (+ 24 B per particle slot)

@@ -202,6 +202,7 @@ XArgs xargs(isf_handle* h) {
     a.g = h->g;
     a.F = h->F;
     a.wp = h->wp;
+    a.kmajor = h->kmajor;
     return a;
 }
 
@@ -269,10 +270,21 @@ int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
     }
     ISF_LAUNCH(h, launch_stencil(ST_DIV, sa, h->stream), "projection div");
     ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "projection x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "projection y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "projection z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "projection y inv");
+    if (int rc = run_poisson_spectral(h, "projection")) return rc;
     ISF_LAUNCH(h, launch_xreal(XR_INV_GAUGE, xa, h->stream), "projection x inv + gauge");
+    return ISF_OK;
+}
+
+// y / z transforms with fac/N between them, on the handle's half spectrum:
+// one plane kernel for a k-major spectrum, three y / z passes otherwise
+int run_poisson_spectral(isf_handle* h, const char* site) {
+    if (h->kmajor) {
+        ISF_LAUNCH(h, launch_poisson_plane(h->g, h->F, 0, 1, h->stream), (std::string(site) + " yz planes").c_str());
+        return ISF_OK;
+    }
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), (std::string(site) + " y fwd").c_str());
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), (std::string(site) + " z fac").c_str());
+    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), (std::string(site) + " y inv").c_str());
     return ISF_OK;
 }
 
@@ -318,6 +330,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     std::vector<char> host;
     fill_grid(p->grid_res, p->physical_size, p->hbar, p->dt, g, host);
     h->wp = half_spectrum_row(g.n[0]);
+    h->kmajor = plane_supported(g.n) ? 1 : 0;
     const size_t total = host.size();
     auto cleanup = [&](int code, const std::string& msg) {
         if (h->F) cudaFree(h->F);
@@ -578,9 +591,7 @@ int isf_poisson_solve(isf_handle* h, const float* f, float* q) {
     xa.rin = f;
     xa.rout = q;
     ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "poisson x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "poisson y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "poisson z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "poisson y inv");
+    if (int rc = run_poisson_spectral(h, "poisson")) return rc;
     ISF_LAUNCH(h, launch_xreal(XR_INV_REAL, xa, h->stream), "poisson x inv");
     return ISF_OK;
 }

@@ -110,9 +110,7 @@ int projection_q(isf_handle* h, const float* psi, float* q) {
     xa.rin = h->f;
     xa.rout = q;
     ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "adj poisson x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "adj poisson y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "adj poisson z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "adj poisson y inv");
+    if (int rc = run_poisson_spectral(h, "adj poisson")) return rc;
     ISF_LAUNCH(h, launch_xreal(XR_INV_REAL, xa, h->stream), "adj poisson x inv");
     return ISF_OK;
 }
@@ -123,9 +121,7 @@ int poisson(isf_handle* h, const float* in, float* out) {
     xa.rin = in;
     xa.rout = out;
     ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "adj poisson x fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FWD, yzhalf(h, 1), h->stream), "adj poisson y fwd");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_FAC, yzhalf(h, 2), h->stream), "adj poisson z fac");
-    ISF_LAUNCH(h, launch_yzpass_c(YZ_INV, yzhalf(h, 1), h->stream), "adj poisson y inv");
+    if (int rc = run_poisson_spectral(h, "adj poisson")) return rc;
     ISF_LAUNCH(h, launch_xreal(XR_INV_REAL, xa, h->stream), "adj poisson x inv");
     return ISF_OK;
 }

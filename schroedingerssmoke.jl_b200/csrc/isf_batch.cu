@@ -87,6 +87,7 @@ struct BatchClass {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     int tiles[ISF_TILE_KINDS] = {1, 1, 1, 1, 1, 1};
+    int kmajor = 0;  // k-major half spectrum, solved plane by plane
     long long bs_F() const { return (long long)wp * g.n[1] * g.n[2]; }
 };
 
@@ -162,6 +163,7 @@ XArgs bx(const BatchClass& c, int groups) {
     a.bs_F = c.bs_F();
     a.bs_r = c.g.N;
     a.groups = groups;
+    a.kmajor = c.kmajor;
     return a;
 }
 
@@ -220,9 +222,13 @@ cudaError_t class_projection(const BatchClass& c, const JetArgs* jets, cudaStrea
     }
     if ((e = launch_stencil(ST_DIV, sa, s)) != cudaSuccess) return e;
     if ((e = launch_xreal(XR_FWD, xa, s)) != cudaSuccess) return e;
-    if ((e = launch_yzpass_c(YZ_FWD, byz(c, true, 1, c.tiles[ISF_TILE_Y_HALF]), s)) != cudaSuccess) return e;
-    if ((e = launch_yzpass_c(YZ_FAC, byz(c, true, 2, c.tiles[ISF_TILE_Z_HALF]), s)) != cudaSuccess) return e;
-    if ((e = launch_yzpass_c(YZ_INV, byz(c, true, 1, c.tiles[ISF_TILE_Y_HALF]), s)) != cudaSuccess) return e;
+    if (c.kmajor) {
+        if ((e = launch_poisson_plane(c.g, c.F, c.bs_F(), c.nsim, s)) != cudaSuccess) return e;
+    } else {
+        if ((e = launch_yzpass_c(YZ_FWD, byz(c, true, 1, c.tiles[ISF_TILE_Y_HALF]), s)) != cudaSuccess) return e;
+        if ((e = launch_yzpass_c(YZ_FAC, byz(c, true, 2, c.tiles[ISF_TILE_Z_HALF]), s)) != cudaSuccess) return e;
+        if ((e = launch_yzpass_c(YZ_INV, byz(c, true, 1, c.tiles[ISF_TILE_Y_HALF]), s)) != cudaSuccess) return e;
+    }
     return launch_xreal(XR_INV_GAUGE, xa, s);
 }
 
@@ -272,6 +278,8 @@ int kind_len(const BatchClass& c, int kind) {
 // a G is a candidate when the kernels exist for it and it divides the work
 bool tile_fits(const BatchClass& c, int kind, int G) {
     if (!grouped_tile_ok(kind_len(c, kind), G)) return false;
+    // a k-major class runs its real x passes ungrouped and has no half-spectrum y / z passes
+    if (c.kmajor && (kind == ISF_TILE_X_REAL || kind == ISF_TILE_Y_HALF || kind == ISF_TILE_Z_HALF)) return G == 1;
     const long long rows = (long long)c.g.n[1] * c.g.n[2];
     switch (kind) {
         case ISF_TILE_X_PSI: return rows % (8LL * G) == 0;
@@ -289,6 +297,10 @@ int tune_class(isf_batch* b, BatchClass& c) {
     for (int kind = 0; kind < ISF_TILE_KINDS && rc == ISF_OK; ++kind) {
         float best = 1e30f;
         int bestG = 1;
+        if (c.kmajor && (kind == ISF_TILE_Y_HALF || kind == ISF_TILE_Z_HALF)) {
+            c.tiles[kind] = 1;
+            continue;
+        }
         for (int G : {1, 2, 4}) {
             if (!tile_fits(c, kind, G)) continue;
             cudaError_t e = cudaSuccess;
@@ -472,6 +484,7 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
         std::vector<char> host;
         fill_grid(c.key.n, c.key.L, c.key.hbar, c.key.dt, c.g, host);
         c.wp = half_spectrum_row(c.g.n[0]);
+        c.kmajor = plane_supported(c.g.n) ? 1 : 0;
         const size_t ns = (size_t)c.nsim;
         if (cudaMalloc(&c.psi, sizeof(float4) * c.g.N * ns) != cudaSuccess ||
             cudaMalloc(&c.F, sizeof(float2) * c.bs_F() * ns) != cudaSuccess ||

@@ -17,6 +17,7 @@ struct isf_handle {
     bool own_stream = false;
     float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
     int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
+    int kmajor = 0;          // the half spectrum is k-major and solved plane by plane (plane_supported)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
     float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
@@ -74,6 +75,8 @@ JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], f
 int run_schroedinger(isf_handle* h, float* psi, bool norm);
 int run_projection(isf_handle* h, float* psi, const JetArgs* jet);
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site);
+// the y / z transforms and the Laplacian multiply of the Poisson solve on h->F
+int run_poisson_spectral(isf_handle* h, const char* site);
 
 // releases the adjoint work buffers (isf_adj.cu)
 void adj_free(isf_handle* h);

@@ -49,6 +49,10 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s);
 cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_psi(int op, const YZArgs& a, cudaStream_t s);
 cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s);
+// the (y, z) plane Poisson solver of a k-major half spectrum (ny == nz in
+// {32, 48, 64, 96, 128}); nsim simulations bs_F elements apart
+bool plane_supported(const int n[3]);
+cudaError_t launch_poisson_plane(const Grid& g, float2* F, long long bs_F, int nsim, cudaStream_t s);
 
 // z-marching stencils of the one-form (k_stencil.cu)
 enum StOp { ST_DIV = 0, ST_VEL = 1 };

@@ -50,6 +50,7 @@ struct XArgs {
     long long bs_psi, bs_F, bs_r;
     const JetArgs* jets;
     int groups;  // pencil groups per CTA (0 or 1: one)
+    int kmajor;  // real x passes: the half spectrum is k-major (see k_xreal)
 };
 
 template <int OP>
@@ -112,30 +113,41 @@ __global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
 //   XR_INV_GAUGE  Z_j = A_j + i B_j (Hermitian extension for j > N/2) ->
 //                 inverse -> q rows (Re, Im) -> psi = gauge(psi (restricted), q)
 //   XR_INV_REAL   the same inverse, q rows to a real output array
-// The half spectrum of row r starts at F + r * wp (wp >= N/2 + 1, padded to
-// whole 16-column tiles for the y / z passes).
+// Half-spectrum layouts:
+//   row-major (KM = false)  row r's spectrum at F + r * wp (wp >= N/2 + 1,
+//                           padded to whole 16-column tiles for the y / z passes)
+//   k-major   (KM = true)   element (k, y, z) at F + (k nz + z) ny + y: one
+//                           contiguous (y, z) plane per k for the plane solver
+//                           (k_poisson_plane); A and B of a row pair are
+//                           neighbours, moved as one 16-byte vector, with the
+//                           lanes running over row pairs.
 enum XROp { XR_FWD = 0, XR_INV_GAUGE = 1, XR_INV_REAL = 2 };
 
-template <int N, int G = 1>
+template <int N, int G = 1, bool KM = false>
 struct XRShape {
     static constexpr int C = 16;
     static constexpr int NT = Plan<N>::NT;
     static constexpr int BLK = G * C * NT;
-    static constexpr size_t SMEM = (size_t)G * N * C * sizeof(float2);
+    // the k-major inverse stages (A, B) of N/2 + 1 k per row pair in the tile
+    static constexpr size_t TILE = (size_t)N * C * sizeof(float2);
+    static constexpr size_t STAGE = (size_t)(N / 2 + 1) * C * sizeof(float4);
+    static constexpr size_t SMEM = (size_t)G * (KM && STAGE > TILE ? STAGE : TILE);
 };
 
-template <int N, int OP, int G>
-__global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
+template <int N, int OP, int G, bool KM = false>
+__global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
     pdl_enter();
     using T = float2;
     constexpr int C = 16;
     constexpr int NT = Plan<N>::NT;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
-    T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
+    T* sm = reinterpret_cast<T*>(smraw + grp * XRShape<N, G, KM>::SMEM / G);
     const int t = lt % NT, q = lt / NT;
-    const long long r0 = 2 * (((long long)blockIdx.x * G + grp) * C + q);
+    const long long rbase = 2 * ((long long)blockIdx.x * G + grp) * C;  // first row of the group
+    const long long r0 = rbase + 2 * q;
     const int wp = a.wp;
+    const int ny = a.g.n[1], nz = a.g.n[2];
     const int sim = blockIdx.y;
     float2* __restrict__ Fs = a.F + sim * a.bs_F;
     T x[Plan<N>::EMAX];
@@ -146,28 +158,62 @@ __global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
         auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
         Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst);
         __syncthreads();
-        float2* __restrict__ A = Fs + r0 * wp;
-        float2* __restrict__ B = A + wp;
+        if constexpr (KM) {
+            // lanes over the row pairs of the group: 16 x 16 B per k
+            float4* __restrict__ F4 = reinterpret_cast<float4*>(Fs);
+            for (int idx = lt; idx < (N / 2 + 1) * C; idx += C * NT) {
+                const int qq = idx % C, k = idx / C;
+                const float2 zk = sm[sidx<C>(k, qq)];
+                const float2 zn = sm[sidx<C>(k == 0 ? 0 : N - k, qq)];
+                const long long r = rbase + 2 * qq;
+                const int y = (int)(r % ny), z = (int)(r / ny);
+                F4[(((long long)k * nz + z) * ny + y) >> 1] =
+                    make_float4(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y), 0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            }
+        } else {
+            float2* __restrict__ A = Fs + r0 * wp;
+            float2* __restrict__ B = A + wp;
 #pragma unroll 1
-        for (int k = t; k <= N / 2; k += NT) {
-            const float2 zk = sm[sidx<C>(k, q)];
-            const float2 zn = sm[sidx<C>(k == 0 ? 0 : N - k, q)];
-            A[k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-            B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            for (int k = t; k <= N / 2; k += NT) {
+                const float2 zk = sm[sidx<C>(k, q)];
+                const float2 zn = sm[sidx<C>(k == 0 ? 0 : N - k, q)];
+                A[k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+            }
         }
     } else {
         const float2* __restrict__ A = Fs + r0 * wp;
         const float2* __restrict__ B = A + wp;
+        // k-major: (A_k, B_k) of every row pair staged in the tile first
+        // (swizzled: conflict free for the lanes over row pairs that fill it
+        // and for the lanes over k that read it)
+        float4* stg = reinterpret_cast<float4*>(sm);
+        if constexpr (KM) {
+            const float4* __restrict__ F4 = reinterpret_cast<const float4*>(Fs);
+            for (int idx = lt; idx < (N / 2 + 1) * C; idx += C * NT) {
+                const int qq = idx % C, k = idx / C;
+                const long long r = rbase + 2 * qq;
+                const int y = (int)(r % ny), z = (int)(r / ny);
+                stg[k * C + (qq ^ (k & (C - 1)))] = F4[(((long long)k * nz + z) * ny + y) >> 1];
+            }
+            __syncthreads();
+        }
         float* __restrict__ rout = a.rout + sim * a.bs_r;
         float4* __restrict__ psi = a.psi + sim * a.bs_psi;
         const bool use_jet = a.use_jet != 0;
         const JetArgs jet = a.jets ? a.jets[sim] : a.jet;
         auto src = [&](int j) -> T {
-            if (j <= N / 2) {
-                const float2 u = A[j], v = B[j];
-                return make_float2(u.x - v.y, u.y + v.x);
+            const int k = j <= N / 2 ? j : N - j;
+            float2 u, v;
+            if constexpr (KM) {
+                const float4 s = stg[k * C + (q ^ (k & (C - 1)))];
+                u = make_float2(s.x, s.y);
+                v = make_float2(s.z, s.w);
+            } else {
+                u = A[k];
+                v = B[k];
             }
-            const float2 u = A[N - j], v = B[N - j];
+            if (j <= N / 2) return make_float2(u.x - v.y, u.y + v.x);
             return make_float2(u.x + v.y, v.x - u.y);
         };
         const long long b0 = r0 * N, b1 = b0 + N;
@@ -179,7 +225,6 @@ __global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
                 static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
                 float4 p0 = psi[b0 + j], p1 = psi[b1 + j];
                 if (use_jet) {
-                    const int ny = a.g.n[1];
                     restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
                     restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
                 }
@@ -187,7 +232,128 @@ __global__ void __launch_bounds__(XRShape<N, G>::BLK) k_xreal(XArgs a) {
                 psi[b1 + j] = gauge4(p1, v.y);
             }
         };
-        Plan<N>::template run<C, +1, false>(x, t, q, sm, a.g.tw[0], src, dst);
+        // k-major: the staging aliases the tile, so the first gather must
+        // complete before the first stage writes the tile
+        Plan<N>::template run<C, +1, KM>(x, t, q, sm, a.g.tw[0], src, dst);
+    }
+}
+
+// ------------------------------------------- Poisson solve on (y, z) planes
+// With the k-major half spectrum, the y and z transforms of one kx are a
+// contiguous N x N plane (ny = nz = N).  One CTA holds the plane in shared
+// memory and runs y forward -> z forward * fac/N, z inverse (register
+// hand-off, Plan::run_spectral) -> y inverse on it, so the plane crosses HBM
+// / L2 once instead of three times.  GROUPS pencil groups of C pencils work
+// side by side, each with its own [N][C] tile; every group runs the same
+// number of rounds (idle in the last one if N / C is not a multiple), so the
+// barriers inside the transforms stay uniform.
+struct PlaneArgs {
+    Grid g;
+    float2* F;       // k-major half spectrum
+    long long bs_F;  // elements between simulations of a batch
+};
+
+#ifndef ISF_PLANE_MAX_THREADS
+#define ISF_PLANE_MAX_THREADS 1024
+#endif
+
+template <int N>
+struct PlaneShape {
+    static constexpr int C = 16;
+    static constexpr int NT = Plan<N>::NT;
+    static constexpr int GT = C * NT;  // threads of one pencil group
+    static constexpr int GMAX = ISF_PLANE_MAX_THREADS / GT > 0 ? ISF_PLANE_MAX_THREADS / GT : 1;
+    static constexpr int GROUPS = GMAX < (N / C) ? GMAX : (N / C);
+    static constexpr int BLK = GROUPS * GT;
+    static constexpr int ROUNDS = (N / C + GROUPS - 1) / GROUPS;
+    static constexpr size_t SMEM = (size_t)N * N * sizeof(float2) + (size_t)GROUPS * N * C * sizeof(float2);
+    static_assert(N % C == 0, "plane width");
+};
+
+template <int N>
+__global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs a) {
+    pdl_enter();
+    using Sh = PlaneShape<N>;
+    constexpr int C = Sh::C, NT = Sh::NT, GT = Sh::GT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float2* plane = reinterpret_cast<float2*>(smraw);
+    const int grp = threadIdx.x / GT, lt = threadIdx.x % GT;
+    float2* tile = plane + N * N + grp * (N * C);
+    const int kx = blockIdx.x;
+    float2* __restrict__ Fp = a.F + blockIdx.y * a.bs_F + (long long)kx * N * N;
+    constexpr int NV = N * N / 2, VIT = (NV + Sh::BLK - 1) / Sh::BLK;  // float4 per plane, per thread
+    {
+        // all of a thread's loads in flight at once
+        const float4* __restrict__ s4 = reinterpret_cast<const float4*>(Fp);
+        float4* p4 = reinterpret_cast<float4*>(plane);
+        float4 v[VIT];
+#pragma unroll
+        for (int it = 0; it < VIT; ++it) {
+            const int i = it * Sh::BLK + threadIdx.x;
+            if (i < NV) v[it] = s4[i];
+        }
+#pragma unroll
+        for (int it = 0; it < VIT; ++it) {
+            const int i = it * Sh::BLK + threadIdx.x;
+            if (i < NV) p4[i] = v[it];
+        }
+    }
+    __syncthreads();
+    float2 x[Plan<N>::EMAX];
+    const float2 zero = make_float2(0.f, 0.f);
+    // y transforms: pencil = row z of the plane, lanes along y
+    auto ysweep = [&](auto sign) {
+        constexpr int S = decltype(sign)::value;
+        const int t = lt % NT, q = lt / NT;
+#pragma unroll 1
+        for (int round = 0; round < Sh::ROUNDS; ++round) {
+            const int z = (round * Sh::GROUPS + grp) * C + q;
+            const bool on = z < N;
+            auto src = [&](int j) -> float2 { return on ? plane[z * N + j] : zero; };
+            auto dst = [&](int j, const float2& v) {
+                if (on) plane[z * N + j] = v;
+            };
+            Plan<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst);
+            __syncthreads();
+        }
+    };
+    ysweep(std::integral_constant<int, -1>());
+    // z: forward, * fac(kx, ky, kz) / N, inverse; pencil = column ky, lanes across ky
+    {
+        const int q = lt % C, t = lt / C;
+        const double sx = a.g.s2[0][kx];
+        const double sc = -0.25 * a.g.invN;
+        const double* __restrict__ s2z = a.g.s2[2];
+#pragma unroll 1
+        for (int round = 0; round < Sh::ROUNDS; ++round) {
+            const int ky = (round * Sh::GROUPS + grp) * C + q;
+            const bool on = ky < N;
+            const int kyc = on ? ky : 0;
+            const double dxo = sx + a.g.s2[1][kyc];
+            const bool zero_line = (kx == 0) && (kyc == 0);
+            auto src = [&](int j) -> float2 { return on ? plane[j * N + ky] : zero; };
+            auto dst = [&](int j, const float2& v) {
+                if (on) plane[j * N + ky] = v;
+            };
+            // fac(k)/N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
+            // (parallel.jl:53-55, 63), as in the y/z pass YZ_FAC
+            auto fmul = [&](int j, const float2& v) -> float2 {
+                const float f = (zero_line && j == 0) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2z[j])));
+                return cscale(v, f);
+            };
+            Plan<N>::template run_spectral<C>(x, t, q, tile, a.g.tw[2], src, fmul, dst);
+            __syncthreads();
+        }
+    }
+    ysweep(std::integral_constant<int, +1>());
+    {
+        float4* __restrict__ d4 = reinterpret_cast<float4*>(Fp);
+        const float4* p4 = reinterpret_cast<const float4*>(plane);
+#pragma unroll
+        for (int it = 0; it < VIT; ++it) {
+            const int i = it * Sh::BLK + threadIdx.x;
+            if (i < NV) d4[i] = p4[i];
+        }
     }
 }
 

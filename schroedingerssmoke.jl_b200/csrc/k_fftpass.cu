@@ -75,6 +75,10 @@ cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
 
 template <int N, int OP>
 static cudaError_t launch_xr_n(const XArgs& a, cudaStream_t s) {
+    if (a.kmajor) {
+        if (a.groups > 1) return cudaErrorInvalidValue;
+        return launch_xr_ng<N, OP, 1, true>(a, s);
+    }
     if constexpr (N <= kMaxGroupedN && grouped_xr_op(OP)) {
         if (a.groups == 2) return launch_xr_ng<N, OP, 2>(a, s);
         if (a.groups == 4) return launch_xr_ng<N, OP, 4>(a, s);
@@ -131,6 +135,44 @@ cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s) {
         case YZ_FWD: return launch_yz_op<float2, YZ_FWD>(a, s);
         case YZ_INV: return launch_yz_op<float2, YZ_INV>(a, s);
         case YZ_FAC: return launch_yz_op<float2, YZ_FAC>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---- the (y, z) plane Poisson solver of the k-major half spectrum
+
+bool plane_supported(const int n[3]) {
+    if (n[1] != n[2]) return false;
+    switch (n[1]) {
+        case 32: case 48: case 64: case 96: case 128:
+            return true;
+        default:
+            return false;
+    }
+}
+
+template <int N>
+static cudaError_t launch_plane_n(const PlaneArgs& a, int nsim, cudaStream_t s) {
+    using Sh = PlaneShape<N>;
+    static std::atomic<unsigned long long> done{0};
+    cudaError_t e = ensure_smem(k_poisson_plane<N>, Sh::SMEM, done);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((unsigned)(a.g.n[0] / 2 + 1), batch_dim(nsim));
+    return launch_pdl(k_poisson_plane<N>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
+}
+
+cudaError_t launch_poisson_plane(const Grid& g, float2* F, long long bs_F, int nsim, cudaStream_t s) {
+    if (!plane_supported(g.n)) return cudaErrorInvalidValue;
+    PlaneArgs a;
+    a.g = g;
+    a.F = F;
+    a.bs_F = bs_F;
+    switch (g.n[1]) {
+        case 32: return launch_plane_n<32>(a, nsim, s);
+        case 48: return launch_plane_n<48>(a, nsim, s);
+        case 64: return launch_plane_n<64>(a, nsim, s);
+        case 96: return launch_plane_n<96>(a, nsim, s);
+        case 128: return launch_plane_n<128>(a, nsim, s);
         default: return cudaErrorInvalidValue;
     }
 }

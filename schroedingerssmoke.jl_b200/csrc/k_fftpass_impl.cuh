@@ -42,16 +42,16 @@ cudaError_t launch_x_ng(const XArgs& a, cudaStream_t s) {
     return launch_pdl(k_xpass<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
-template <int N, int OP, int G>
+template <int N, int OP, int G, bool KM = false>
 cudaError_t launch_xr_ng(const XArgs& a, cudaStream_t s) {
-    using Sh = XRShape<N, G>;
+    using Sh = XRShape<N, G, KM>;
     static std::atomic<unsigned long long> done{0};
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
     if (rows % (2 * Sh::C * G) != 0) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_smem(k_xreal<N, OP, G>, Sh::SMEM, done);
+    cudaError_t e = ensure_smem(k_xreal<N, OP, G, KM>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)(rows / (2 * Sh::C * G)), batch_dim(a.nsim));
-    return launch_pdl(k_xreal<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
+    return launch_pdl(k_xreal<N, OP, G, KM>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 template <int N, class T, int OP, int G>
