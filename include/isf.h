@@ -149,6 +149,11 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
  * first of them and [4..11] its cell indices, two neighbour indices and strides.
  * Synchronises the handle's stream. */
 ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);
+/* The same counters copied asynchronously: the copy of the first n (1..16)
+ * into host_out (pinned host memory for a truly asynchronous copy) is queued
+ * on the handle's stream after the work already queued, and the reset after
+ * it; host_out is valid once the stream is synchronised. */
+ISF_API int isf_counters_async(isf_handle* h, uint64_t* host_out, int32_t n, int32_t reset);
 
 /* ---- allocation-free entry point (no counterpart in the reference) -------
  * The real part of poisson_solve (the same result as isf_poisson_solve) for

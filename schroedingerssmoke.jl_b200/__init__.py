@@ -138,6 +138,14 @@ class ISF:
         return {"clamp_events": int(out[0]), "live": int(out[1]), "check_failures": int(out[2]),
                 "first_bad_index": int(out[3]), "first_bad_context": [int(v) for v in out[4:12]]}
 
+    def counters_async(self, out: torch.Tensor, reset: bool = False):
+        """Queue a copy of the advection counters [clamp events, live] into
+        `out` (a pinned int64 CPU tensor of 2+ entries) on the handle's stream;
+        valid after sync()."""
+        if out.device.type != "cpu" or out.dtype != torch.int64 or out.numel() < 2:
+            raise ISFError(_lib.ISF_ERR_INVALID, "counters_async needs an int64 CPU tensor of 2+ entries")
+        check(self.L.isf_counters_async(self.h, C.c_void_p(out.data_ptr()), 2, int(reset)), self.h)
+
     def launch_count(self) -> int:
         out = C.c_uint64()
         check(self.L.isf_launch_count(self.h, C.byref(out)), self.h)

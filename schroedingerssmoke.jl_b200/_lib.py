@@ -21,7 +21,7 @@ EXPORTS = (
     "isf_memcpy_h2d", "isf_memcpy_d2h", "isf_grid_info", "isf_schroedinger_flow", "isf_normalize_psi",
     "isf_pressure_project", "isf_velocity_one_form", "isf_staggered_sharp", "isf_get_velocity",
     "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
-    "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters", "isf_profile_start",
+    "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters", "isf_counters_async", "isf_profile_start",
     "isf_profile_stop", "isf_profile_sites", "isf_profile_get", "isf_launch_count", "isf_poisson_solve_static",
     "isf_static_last_error", "isf_batch_create", "isf_batch_destroy", "isf_batch_last_error",
     "isf_batch_set_psi", "isf_batch_get_psi", "isf_batch_set_particles", "isf_batch_get_particles",
@@ -148,6 +148,7 @@ def load(path: str | None = None):
         "isf_poisson_solve": [vp, vp, vp],
         "isf_fft3": [vp, vp, i32],
         "isf_counters": [vp, C.POINTER(C.c_uint64), i32, i32],
+        "isf_counters_async": [vp, vp, i32, i32],
         "isf_profile_start": [vp],
         "isf_profile_stop": [vp],
         "isf_profile_sites": [vp, C.POINTER(C.c_int32)],

@@ -677,4 +677,13 @@ int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset) {
     return ISF_OK;
 }
 
+int isf_counters_async(isf_handle* h, uint64_t* host_out, int32_t n, int32_t reset) {
+    ISF_ENTER(h);
+    if (n < 1 || n > 16 || !host_out) return fail(h, ISF_ERR_INVALID, "isf_counters_async: n must be 1..16");
+    ISF_CUDA(h, cudaMemcpyAsync(host_out, h->counters, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, h->stream),
+             "counters");
+    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * 16, h->stream), "counters reset");
+    return ISF_OK;
+}
+
 }  // extern "C"

@@ -18,13 +18,20 @@ namespace isf {
 
 namespace {
 
+// z planes per CTA: the div stencil (which also computes the tile's halo
+// angles) amortises its prologue over more planes than the one-form stencil
 #ifndef ISF_ST_SZ
 #define ISF_ST_SZ 8
+#endif
+#ifndef ISF_ST_SZ_VEL
+#define ISF_ST_SZ_VEL 4
 #endif
 #ifndef ISF_ST_RPT
 #define ISF_ST_RPT 2
 #endif
-constexpr int BX = 32, TY = 8, RPT = ISF_ST_RPT, BY = TY * RPT, SZ = ISF_ST_SZ;  // 256 threads
+constexpr int BX = 32, TY = 8, RPT = ISF_ST_RPT, BY = TY * RPT;  // 256 threads
+template <int OP>
+constexpr int planes_per_cta() { return OP == ST_DIV ? ISF_ST_SZ : ISF_ST_SZ_VEL; }
 constexpr int TW = BX + 2, TH = BY + 2, TILE = TW * TH;        // padded tile
 constexpr int LPT = (TILE + BX * TY - 1) / (BX * TY);           // tile loads per thread
 
@@ -37,6 +44,7 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int tid = threadIdx.x, tx = tid & (BX - 1), ty = tid / BX;
     // blockIdx.z = simulation * (z chunks) + z chunk
+    constexpr int SZ = planes_per_cta<OP>();
     const int zchunks = (nz + SZ - 1) / SZ;
     const int sim = blockIdx.z / zchunks;
     const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = (blockIdx.z - sim * zchunks) * SZ;
@@ -205,8 +213,9 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
 
 cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
     const int nsim = a.nsim > 1 ? a.nsim : 1;
+    const int sz = op == ST_DIV ? planes_per_cta<ST_DIV>() : planes_per_cta<ST_VEL>();
     dim3 grid((unsigned)((a.g.n[0] + BX - 1) / BX), (unsigned)((a.g.n[1] + BY - 1) / BY),
-              (unsigned)(((a.g.n[2] + SZ - 1) / SZ) * nsim));
+              (unsigned)(((a.g.n[2] + sz - 1) / sz) * nsim));
     if (op == ST_DIV) return launch_pdl(k_stencil<ST_DIV>, grid, dim3(BX * TY), 0, s, a);
     if (op == ST_VEL) return launch_pdl(k_stencil<ST_VEL>, grid, dim3(BX * TY), 0, s, a);
     return cudaErrorInvalidValue;

@@ -257,3 +257,23 @@ def test_invalid_arguments(isfpkg):
     parts = torch.zeros((10, 3), device="cuda")
     with pytest.raises(isfpkg.ISFError):
         isfpkg.add_particles(isf, parts, range(0, 11), (0, 0, 0), 0.1)
+
+
+def test_counters_async_match(isfpkg):
+    """isf_counters_async queues the same counters isf_counters reads, behind
+    the queued work, and resets them when asked."""
+    L, dims = (4, 2, 2), (64, 32, 32)
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    rng = np.random.default_rng(8)
+    isf.velocity = cuda(np.stack([smooth_field(dims, rng, scale=0.5) for _ in range(3)], axis=-1))
+    parts = cuda(rng.uniform(0.1, 0.9, (5000, 3)) * np.asarray(L))
+    parts[:700] = -1.0
+    out = torch.zeros((2, 2), dtype=torch.int64).pin_memory()
+    isfpkg.staggered_advect(parts, isf)
+    isf.counters_async(out[0], reset=True)
+    isfpkg.staggered_advect(parts, isf)
+    isf.counters_async(out[1], reset=False)
+    isf.sync()
+    assert int(out[0, 1]) == 4300 and int(out[1, 1]) <= 4300
+    c = isf.counters(reset=True)
+    assert c["live"] == int(out[1, 1]) and c["clamp_events"] == int(out[1, 0])
