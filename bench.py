@@ -68,6 +68,24 @@ STEP_BYTES_PER_CELL = 196      # no-jet step: 64 + 36 + 32 + 52 + 12
 STEP_BYTES_PER_PARTICLE = 24   # position read + write
 
 
+def rank_max(x: float, world: int, device) -> float:
+    """The maximum of x over the ranks of the process group (x itself on one
+    rank): the job is as slow as its slowest replica."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(steps: int, ms_max: float, world: int) -> float:
+    """Steps per second of the whole job: every replica ran `steps` steps
+    within ms_max milliseconds (the max over ranks)."""
+    return world * steps / (ms_max / 1000.0)
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -361,11 +379,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, world, f"cuda:{local}")
 
     # ---- device-resident timing
     for _ in range(args.warmup):
@@ -386,7 +400,7 @@ def main():
     ms = e0.elapsed_time(e1)
     gpu_launches = isf.launch_count() - launches0
     ms = max_over_ranks(ms)
-    value = world * args.steps / (ms / 1000.0)
+    value = whole_job_rate(args.steps, ms, world)
     ms_per_step = ms / args.steps
 
     # ---- per-launch-site timing over a second pass of the same window
@@ -443,7 +457,7 @@ def main():
         live = int(res[-1, 1])
         ems = max_over_ranks(f0.elapsed_time(f1))
         state = (h_psi.numel() + h_parts.numel()) * 4
-        e2e = {"value": world * args.steps / (ems / 1000.0), "unit": UNIT,
+        e2e = {"value": whole_job_rate(args.steps, ems, world), "unit": UNIT,
                "h2d_bytes_per_step": state / args.steps, "d2h_bytes_per_step": 16 + state / args.steps,
                "what": "isf_memcpy_h2d of psi0 + particles, K x (isf_step + 16-byte counter read into pinned "
                        "host memory, isf_counters_async), isf_memcpy_d2h of psi + particles",

@@ -43,6 +43,18 @@ enum {
     ISF_ERR_INVALID = 1,     /* bad argument or unsupported size */
     ISF_ERR_CUDA = 2,        /* CUDA runtime error (message has the CUDA text) */
     ISF_ERR_NOMEM = 3,       /* device allocation failed */
+    ISF_ERR_NAN = 4,         /* isf_step with ISF_FLAG_CHECK_NAN found a non-finite psi */
+};
+
+/* isf_params.flags */
+enum {
+    /* staggered_velocity weights divided by d (parallel.jl:238 leaves them in
+     * units of length, as does MatlabPort.jl:259-261): the interpolation
+     * becomes the usual bilinear one */
+    ISF_FLAG_NORMALIZED_WEIGHTS = 1,
+    /* isf_step checks psi for non-finite values after the step (a
+     * reduction and a synchronisation per step) and returns ISF_ERR_NAN */
+    ISF_FLAG_CHECK_NAN = 2,
 };
 
 /* jet phase: reference tuple_dot(k, x) = sum(k .+ x) (src/particles.jl:1,15)
@@ -61,7 +73,7 @@ typedef struct isf_params {
     float hbar;               /* reduced Planck constant */
     float dt;                 /* time step */
     int32_t device;           /* CUDA device ordinal */
-    int32_t flags;            /* reserved, must be 0 */
+    int32_t flags;            /* ISF_FLAG_* bits (0: the reference's semantics) */
     void* stream;             /* cudaStream_t to run on, or NULL: the handle makes its own */
 } isf_params;
 
@@ -146,7 +158,9 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
 /* First n (<= 16) counters of the advections since the last reset: [0] clamp
  * events (staggered_velocity index rounded to n+1), [1] live particles; in a
  * bounds-checking build (-DISF_CHECK) [2] rejected gather indices, [3] the
- * first of them and [4..11] its cell indices, two neighbour indices and strides.
+ * first of them and [4..11] its cell indices, two neighbour indices and strides;
+ * [15] non-finite psi cells after the last isf_step of a handle made with
+ * ISF_FLAG_CHECK_NAN.
  * Synchronises the handle's stream. */
 ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);
 /* The same counters copied asynchronously: the copy of the first n (1..16)

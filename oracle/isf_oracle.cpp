@@ -210,6 +210,7 @@ struct Orc {
     std::vector<R> f, vel;         // vel: AoS, 3 per cell
     std::vector<C> psi1, psi2;     // temporaries (parallel.jl:31-32)
     long clamp_events = 0;         // staggered_velocity index == n+1 events
+    bool norm_w = false;           // weights divided by d (the normalized-weights flag; the reference does not)
 
     long idx(long x, long y, long z) const { return x + (long)n[0] * (y + (long)n[1] * z); }
 
@@ -439,6 +440,7 @@ struct Orc {
             i[a] = ii;
             ip[a] = (ii + 1) % n[a];
             w[a] = p[a] - (R)ii * d[a];
+            if (norm_w) w[a] = w[a] / d[a];
             if (margin) {
                 double fr = (double)q - std::floor((double)q);
                 double mg = std::min(fr, 1.0 - fr);
@@ -643,6 +645,8 @@ void orc_velocity_one_form(void* h, const void* psi, double hbar) {
     ORC_DISPATCH(h, o.velocity_one_form((const R*)psi, (R)hbar));
 }
 void orc_div(void* h) { ORC_DISPATCH(h, o.div()); }
+// staggered_velocity with weights divided by d (on != 0) or as parallel.jl:238 (0)
+void orc_set_normalized_weights(void* h, int on) { ORC_DISPATCH(h, o.norm_w = on != 0); }
 void orc_poisson_solve(void* h) { ORC_DISPATCH(h, o.poisson_solve()); }
 void orc_gauge(void* h, void* psi) { ORC_DISPATCH(h, o.gauge((R*)psi)); }
 void orc_pressure_project(void* h, void* psi) { ORC_DISPATCH(h, o.pressure_project((R*)psi)); }

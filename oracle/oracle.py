@@ -64,6 +64,7 @@ def lib():
         L.orc_create.restype = vp
         L.orc_create.argtypes = [i32, ip, ip, f32, f32]
         L.orc_destroy.argtypes = [vp]
+        L.orc_set_normalized_weights.argtypes = [vp, i32]
         L.orc_num_threads.restype = i32
         L.orc_set_num_threads.argtypes = [i32]
         for name in ["orc_fft3"]:
@@ -108,7 +109,7 @@ class Oracle:
     oracle promotes those exact values.
     """
 
-    def __init__(self, physical_size, dims, hbar, dt, prec: int = 64):
+    def __init__(self, physical_size, dims, hbar, dt, prec: int = 64, normalized_weights: bool = False):
         self.L = lib()
         self.prec = prec
         self.dtype = np.float64 if prec == 64 else np.float32
@@ -122,6 +123,8 @@ class Oracle:
         self.h = self.L.orc_create(prec, d, s, self.hbar, self.dt)
         if not self.h:
             raise ValueError(f"unsupported grid {self.dims} (sizes must be 2^a 3^b)")
+        if normalized_weights:
+            self.L.orc_set_normalized_weights(self.h, 1)
         self.nx, self.ny, self.nz = self.dims
         self.N = self.nx * self.ny * self.nz
         self.d = tuple(self.dtype(L) / self.dtype(n) for L, n in zip(self.physical_size, self.dims))

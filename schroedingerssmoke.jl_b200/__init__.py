@@ -20,13 +20,14 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, PHASE_DOT, PHASE_REFERENCE_SUM, IsfParams,
-                   IsfStepArgs, ISFError, check, f3)
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
+                   PHASE_REFERENCE_SUM, IsfParams, IsfStepArgs, ISFError, check, f3)
 
 __all__ = [
     "ISF", "ISFBatch", "ISFError", "ParticleLoss", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
     "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
-    "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER",
+    "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER", "FLAG_NORMALIZED_WEIGHTS",
+    "FLAG_CHECK_NAN",
 ]
 
 
@@ -43,7 +44,7 @@ class ISF:
     (src/parallel.jl:41-98): grid, d, velocity and the spectral tables live on
     the device of `device`."""
 
-    def __init__(self, physical_size, dims, hbar, dt, device: int = 0):
+    def __init__(self, physical_size, dims, hbar, dt, device: int = 0, flags: int = 0):
         if not torch.cuda.is_available():
             raise ISFError(_lib.ISF_ERR_CUDA, "no CUDA device: libisf has no CPU path")
         self.L = _lib.load()
@@ -53,7 +54,7 @@ class ISF:
         p.hbar = float(hbar)
         p.dt = float(dt)
         p.device = int(device)
-        p.flags = 0
+        p.flags = int(flags)
         p.stream = None
         h = C.c_void_p()
         check(self.L.isf_create(C.byref(p), C.byref(h)))

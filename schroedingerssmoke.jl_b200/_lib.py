@@ -11,7 +11,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libisf.so")
 
-ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM = 0, 1, 2, 3
+ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM, ISF_ERR_NAN = 0, 1, 2, 3, 4
+FLAG_NORMALIZED_WEIGHTS, FLAG_CHECK_NAN = 1, 2
 PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
 EMIT_RING, EMIT_DISC, EMIT_CYLINDER = 0, 1, 2
 

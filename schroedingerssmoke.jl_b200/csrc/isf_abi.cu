@@ -128,8 +128,8 @@ bool check_params(const isf_params* p, std::string& why) {
         why = "hbar and dt must be finite, dt > 0";
         return false;
     }
-    if (p->flags != 0) {
-        why = "flags must be 0";
+    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN)) {
+        why = "unknown flags";
         return false;
     }
     return true;
@@ -331,6 +331,8 @@ int isf_create(const isf_params* p, isf_handle** out) {
     fill_grid(p->grid_res, p->physical_size, p->hbar, p->dt, g, host);
     h->wp = half_spectrum_row(g.n[0]);
     h->kmajor = plane_supported(g.n) ? 1 : 0;
+    h->flags = p->flags;
+    g.norm_w = (p->flags & ISF_FLAG_NORMALIZED_WEIGHTS) ? 1 : 0;
     const size_t total = host.size();
     auto cleanup = [&](int code, const std::string& msg) {
         if (h->F) cudaFree(h->F);
@@ -574,6 +576,16 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     rc = run_one_form(h, psi, h->g.hbar, 1, "step one_form");
     if (rc) return rc;
     if (np > 0) ISF_LAUNCH(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "step advect");
+    if (h->flags & ISF_FLAG_CHECK_NAN) {
+        // counters[15]: non-finite psi cells after this step
+        ISF_CUDA(h, cudaMemsetAsync(h->counters + 15, 0, sizeof(unsigned long long), h->stream), "nan check");
+        ISF_LAUNCH(h, launch_count_nonfinite(h->g, reinterpret_cast<const float4*>(psi), h->counters + 15, h->stream),
+                   "step nan check");
+        unsigned long long bad = 0;
+        ISF_CUDA(h, cudaMemcpyAsync(&bad, h->counters + 15, sizeof(bad), cudaMemcpyDeviceToHost, h->stream), "nan check");
+        ISF_CUDA(h, cudaStreamSynchronize(h->stream), "nan check");
+        if (bad) return fail(h, ISF_ERR_NAN, "isf_step: " + std::to_string(bad) + " psi cells are not finite");
+    }
     return ISF_OK;
 }
 

@@ -33,6 +33,7 @@ struct Grid {
     double invN;            // 1 / N
     int pnx, pnxy;          // strides of the padded velocity planes: nx+1 (rounded up to the row alignment), pnx (ny+1)
     long long NP;           // cells of one padded velocity plane
+    int norm_w;             // staggered interpolation weights divided by d (ISF_FLAG_NORMALIZED_WEIGHTS)
 };
 
 // index of cell (x, y, z), 0 <= x <= nx etc., in a padded velocity plane

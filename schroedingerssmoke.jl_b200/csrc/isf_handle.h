@@ -17,6 +17,7 @@ struct isf_handle {
     bool own_stream = false;
     float2* F = nullptr;     // Poisson half spectrum (wp x ny x nz complex), N allocated
     int wp = 0;              // padded half-spectrum row: round_up(nx/2 + 1, 16)
+    int flags = 0;           // ISF_FLAG_* of isf_create
     int kmajor = 0;          // the half spectrum is k-major and solved plane by plane (plane_supported)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
     float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP

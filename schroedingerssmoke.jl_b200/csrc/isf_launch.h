@@ -82,6 +82,7 @@ cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s
 cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s);
 cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s);
 cudaError_t launch_scale_c(const Grid& g, float2* a, float s, cudaStream_t st);
+cudaError_t launch_count_nonfinite(const Grid& g, const float4* psi, unsigned long long* count, cudaStream_t s);
 
 // particles (k_particles.cu); slot indices are 32-bit: 3 * np < 2^31
 constexpr long long kMaxParticles = 715827882LL;

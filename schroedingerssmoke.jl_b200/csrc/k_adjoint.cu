@@ -278,7 +278,7 @@ struct Sample {
     float3 u;
 };
 
-template <bool POW2>
+template <bool POW2, bool NORMW>
 __device__ __forceinline__ void stag_sample(const AdvConst& k, float3 pt, Sample& S) {
     float P[3] = {pt.x, pt.y, pt.z};
     const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
@@ -294,6 +294,7 @@ __device__ __forceinline__ void stag_sample(const AdvConst& k, float3 pt, Sample
         ii = max(min(ii, k.nm[a]), 0);
         i[a] = ii;
         S.w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, k.d[a]));
+        if (NORMW) S.w[a] = __fdiv_rn(S.w[a], k.d[a]);
     }
     const int sy = k.pnx, sz = k.pnxy;
     const int c000 = i[0] + sy * i[1] + sz * i[2];
@@ -319,6 +320,7 @@ __device__ __forceinline__ void stag_sample(const AdvConst& k, float3 pt, Sample
 
 // adjoint of one sample: ub = cotangent of u; returns the cotangent of the
 // sample point and scatters ub times the weights into the velocity planes
+template <bool NORMW>
 __device__ __forceinline__ float3 stag_sample_adj(const AdvConst& k, const Sample& S, float3 ub, float* ubx, float* uby,
                                                   float* ubz) {
     const float wx = S.w[0], wy = S.w[1], wz = S.w[2];
@@ -334,6 +336,11 @@ __device__ __forceinline__ float3 stag_sample_adj(const AdvConst& k, const Sampl
     pb.x = ub.y * duy_dwx + ub.z * duz_dwx;
     pb.y = ub.x * dux_dwy + ub.z * duz_dwy;
     pb.z = ub.x * dux_dwz + ub.y * duy_dwz;
+    if (NORMW) {  // w = (p - i d) / d
+        pb.x *= k.dinv[0];
+        pb.y *= k.dinv[1];
+        pb.z *= k.dinv[2];
+    }
     const int sy = k.pnx, sz = k.pnxy;
     const int c000 = S.c000, c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
     if (ub.x != 0.f) {
@@ -367,7 +374,7 @@ __device__ __forceinline__ float3 f3scale(float3 a, float s) { return make_float
 // of the positions before it (parts, the positions the forward step started
 // from); the cotangent of the velocity planes is added into ubar.  A slot
 // outside the open box was set to (-1,-1,-1): its cotangent is 0.
-template <bool POW2>
+template <bool POW2, bool NORMW>
 __global__ void __launch_bounds__(256) k_adj_advect(Grid g, const float* __restrict__ parts, float* __restrict__ lam,
                                                     int np, const float* __restrict__ vel, float* __restrict__ ubar) {
     const AdvConst kc = adv_const(g, vel);
@@ -384,31 +391,31 @@ __global__ void __launch_bounds__(256) k_adj_advect(Grid g, const float* __restr
             continue;
         }
         Sample S1, S2, S3, S4;
-        stag_sample<POW2>(kc, p, S1);
+        stag_sample<POW2, NORMW>(kc, p, S1);
         const float3 k1 = S1.u;
         float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-        stag_sample<POW2>(kc, q, S2);
+        stag_sample<POW2, NORMW>(kc, q, S2);
         const float3 k2 = S2.u;
         q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-        stag_sample<POW2>(kc, q, S3);
+        stag_sample<POW2, NORMW>(kc, q, S3);
         const float3 k3 = S3.u;
         q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-        stag_sample<POW2>(kc, q, S4);
+        stag_sample<POW2, NORMW>(kc, q, S4);
         // reverse of p' = p + dt/6 (k1 + 2 k2 + 2 k3 + k4)
         const float3 L = make_float3(lam[3 * k], lam[3 * k + 1], lam[3 * k + 2]);
         float3 pb = L;
         float3 kb1 = f3scale(L, s6), kb2 = f3scale(L, 2.f * s6), kb3 = f3scale(L, 2.f * s6);
         const float3 kb4 = f3scale(L, s6);
-        float3 qb = stag_sample_adj(kc, S4, kb4, ubx, uby, ubz);  // q4 = p + dt k3
+        float3 qb = stag_sample_adj<NORMW>(kc, S4, kb4, ubx, uby, ubz);  // q4 = p + dt k3
         pb = f3add(pb, qb);
         kb3 = f3add(kb3, f3scale(qb, dt));
-        qb = stag_sample_adj(kc, S3, kb3, ubx, uby, ubz);  // q3 = p + dt/2 k2
+        qb = stag_sample_adj<NORMW>(kc, S3, kb3, ubx, uby, ubz);  // q3 = p + dt/2 k2
         pb = f3add(pb, qb);
         kb2 = f3add(kb2, f3scale(qb, 0.5f * dt));
-        qb = stag_sample_adj(kc, S2, kb2, ubx, uby, ubz);  // q2 = p + dt/2 k1
+        qb = stag_sample_adj<NORMW>(kc, S2, kb2, ubx, uby, ubz);  // q2 = p + dt/2 k1
         pb = f3add(pb, qb);
         kb1 = f3add(kb1, f3scale(qb, 0.5f * dt));
-        qb = stag_sample_adj(kc, S1, kb1, ubx, uby, ubz);  // k1 at p
+        qb = stag_sample_adj<NORMW>(kc, S1, kb1, ubx, uby, ubz);  // k1 at p
         pb = f3add(pb, qb);
         lam[3 * k] = pb.x;
         lam[3 * k + 1] = pb.y;
@@ -519,10 +526,14 @@ cudaError_t launch_adj_advect(const Grid& g, const float* parts, float* lam, lon
     if (np <= 0) return cudaSuccess;
     if (np > kMaxParticles) return cudaErrorInvalidValue;
     const unsigned b = grid_n(np, 256);
-    if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
-        k_adj_advect<true><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
-    else
-        k_adj_advect<false><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
+    const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
+    if (g.norm_w) {
+        if (pow2) k_adj_advect<true, true><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
+        else k_adj_advect<false, true><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
+    } else {
+        if (pow2) k_adj_advect<true, false><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
+        else k_adj_advect<false, false><<<b, 256, 0, s>>>(g, parts, lam, (int)np, vel, ubar);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_loss(const float* x, const float* y, float* lam, long long np, double* loss, cudaStream_t s) {

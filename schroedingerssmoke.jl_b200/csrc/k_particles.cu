@@ -96,7 +96,7 @@ __device__ __forceinline__ int checked(const AdvConst& k, int c, unsigned long l
 // planes.  Interpolation weights are the reference's unnormalised
 // w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
 // clamped to the last cell and counted.
-template <bool POW2>
+template <bool POW2, bool NORMW>
 __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigned& clamps, unsigned long long* chk) {
     float P[3] = {pt.x, pt.y, pt.z};
     // mod.(point, ph_size): identity for points inside the box (the common case)
@@ -115,6 +115,7 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
         ii = max(min(ii, k.nm[a]), 0);
         i[a] = ii;
         w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, k.d[a]));
+        if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
     }
     (void)chk;
     // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell
@@ -143,7 +144,7 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
 // counters[0] accumulates clamp events, counters[1] live particles.
 // A batch launch advects simulation s = blockIdx.y: slots parts + s * 3 np,
 // velocity vel + s * bs_vel, counters + s * kCounterStride.
-template <bool POW2>
+template <bool POW2, bool NORMW>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters, long long bs_vel) {
@@ -162,13 +163,13 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
         if (inside) {
             ++live;
             // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
-            const float3 k1 = stag_vel<POW2>(kc, p, clamps, chk);
+            const float3 k1 = stag_vel<POW2, NORMW>(kc, p, clamps, chk);
             float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-            const float3 k2 = stag_vel<POW2>(kc, q, clamps, chk);
+            const float3 k2 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
             q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-            const float3 k3 = stag_vel<POW2>(kc, q, clamps, chk);
+            const float3 k3 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
             q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-            const float3 k4 = stag_vel<POW2>(kc, q, clamps, chk);
+            const float3 k4 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
             p.x = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
             p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
             p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
@@ -232,16 +233,19 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
         int dev = 0, sms = 0, per = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false>, blk, 0) != cudaSuccess || per < 1)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false, false>, blk, 0) != cudaSuccess || per < 1)
             return cudaErrorInvalidValue;
         resident = sms * per;
     }
     long long b = (np + blk - 1) / blk;
     if (b > resident) b = resident;
     const dim3 grid((unsigned)b, (unsigned)nsim);
-    if (g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2])
-        return launch_pdl(k_advect<true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
-    return launch_pdl(k_advect<false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
+    const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
+    if (g.norm_w)
+        return pow2 ? launch_pdl(k_advect<true, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel)
+                    : launch_pdl(k_advect<false, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
+    return pow2 ? launch_pdl(k_advect<true, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel)
+                : launch_pdl(k_advect<false, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
 }
 
 }  // namespace isf

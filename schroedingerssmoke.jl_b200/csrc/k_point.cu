@@ -101,6 +101,23 @@ __global__ void k_scale_c(float2* __restrict__ a, long long N, float s) {
         a[c] = cscale(a[c], s);
 }
 
+// cells of psi with a non-finite component, added into *count
+__global__ void k_count_nonfinite(const float4* __restrict__ psi, long long N, unsigned long long* __restrict__ count) {
+    unsigned n = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        const float4 v = psi[c];
+        n += (isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w)) ? 0u : 1u;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(count, (unsigned long long)n);
+}
+
+cudaError_t launch_count_nonfinite(const Grid& g, const float4* psi, unsigned long long* count, cudaStream_t s) {
+    k_count_nonfinite<<<grid_for(g.N, 256), 256, 0, s>>>(psi, g.N, count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scale_c(const Grid& g, float2* a, float s, cudaStream_t st) {
     k_scale_c<<<grid_for(g.N, 256), 256, 0, st>>>(a, g.N, s);
     return cudaGetLastError();

@@ -133,13 +133,14 @@ def test_adj_velocity_one_form_with_sharp(isfpkg, setup):
     assert close(dot(host(t), u), g), (dot(host(t), u), g)
 
 
+@pytest.mark.parametrize("norm", [False, True])
 @pytest.mark.parametrize("grid", [((4, 2, 2), (32, 16, 16)), ((5, 2, 2), (48, 16, 16))])
-def test_adj_staggered_advect(isfpkg, oracle_mod, grid):
-    """Power-of-two and general cell sizes; cotangents of the positions and
-    of the velocity planes."""
+def test_adj_staggered_advect(isfpkg, oracle_mod, grid, norm):
+    """Power-of-two and general cell sizes, the reference's and normalised
+    weights; cotangents of the positions and of the velocity planes."""
     Lg, dims = grid
-    isf = isfpkg.ISF(Lg, dims, HBAR, DT)
-    orc = oracle_mod.Oracle(Lg, dims, HBAR, DT)
+    isf = isfpkg.ISF(Lg, dims, HBAR, DT, flags=isfpkg.FLAG_NORMALIZED_WEIGHTS if norm else 0)
+    orc = oracle_mod.Oracle(Lg, dims, HBAR, DT, normalized_weights=norm)
     rng = np.random.default_rng(6)
     v = np.stack([smooth_field(dims, rng, scale=0.8) for _ in range(3)], axis=-1)
     v = f32(v)

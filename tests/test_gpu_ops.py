@@ -277,3 +277,42 @@ def test_counters_async_match(isfpkg):
     assert int(out[0, 1]) == 4300 and int(out[1, 1]) <= 4300
     c = isf.counters(reset=True)
     assert c["live"] == int(out[1, 1]) and c["clamp_events"] == int(out[1, 0])
+
+
+@pytest.mark.parametrize("L,dims", [((4, 2, 2), (64, 32, 32)), ((5, 2, 2), (48, 32, 32))])
+def test_staggered_advect_normalized_weights(isfpkg, oracle_mod, L, dims):
+    """ISF_FLAG_NORMALIZED_WEIGHTS: the staggered weights divided by d, against
+    the oracle with the same switch (power-of-two and general d)."""
+    isf = isfpkg.ISF(L, dims, HBAR, DT, flags=isfpkg.FLAG_NORMALIZED_WEIGHTS)
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT, normalized_weights=True)
+    rng = np.random.default_rng(17)
+    vel = np.stack([smooth_field(dims, rng, scale=0.8) + 0.5 for _ in range(3)], axis=-1)
+    P = 20000
+    parts64 = (rng.uniform(0, 1, (P, 3)) * np.asarray(L, np.float64)).astype(np.float32).astype(np.float64)
+    isf.velocity = cuda(vel)
+    orc.set_velocity(vel.astype(np.float32).astype(np.float64))
+    parts = cuda(parts64)
+    isfpkg.staggered_advect(parts, isf)
+    po, margin = orc.staggered_advect(parts64.copy(), margin=True)
+    err = np.abs(host(parts) - po).max(axis=1) / min(L)
+    near_face = margin < 1e-4
+    assert (err[~near_face] < 1e-5).all(), err[~near_face].max()
+    # the weights matter: the reference's unnormalised weights give other positions
+    ref = oracle_mod.Oracle(L, dims, HBAR, DT)
+    ref.set_velocity(vel.astype(np.float32).astype(np.float64))
+    assert np.abs(ref.staggered_advect(parts64.copy()) - po).max() > 1e-3
+
+
+def test_step_nan_check(isfpkg):
+    """ISF_FLAG_CHECK_NAN: a non-finite psi cell makes isf_step fail with
+    ISF_ERR_NAN; a finite state steps normally."""
+    L, dims = (4, 2, 2), (32, 16, 16)
+    isf = isfpkg.ISF(L, dims, HBAR, DT, flags=isfpkg.FLAG_CHECK_NAN)
+    psi = cuda(smooth_psi(dims, 3))
+    isfpkg.step(isf, psi, None, None)
+    psi[3, 2, 1, 0] = float("nan")
+    with pytest.raises(isfpkg.ISFError, match="not finite") as e:
+        isfpkg.step(isf, psi, None, None)
+    assert e.value.code == 4
+    with pytest.raises(isfpkg.ISFError, match="unknown flags"):
+        isfpkg.ISF(L, dims, HBAR, DT, flags=64)
