@@ -394,6 +394,7 @@ def main():
     e0.record(s)
     for _ in range(args.steps):
         pkg.step(isf, psi, parts, None)
+    isf.join()  # the last step's advection, queued on the particle stream
     e1.record(s)
     e1.synchronize()
     clk = clocks.stop()

@@ -102,10 +102,19 @@ ISF_API int isf_destroy(isf_handle* h);
 /* Message of the last failed call on h (or of the last failed isf_create when h is NULL). */
 ISF_API const char* isf_last_error(const isf_handle* h);
 /* The stream the handle's work runs on.  Without a caller stream, isf_create
- * makes a blocking stream, which is ordered with the legacy default stream. */
+ * makes a blocking stream, which is ordered with the legacy default stream,
+ * and a second blocking stream for the particle work of isf_step (emission
+ * and advection), which then overlaps the next step's psi passes.  Every
+ * entry point except isf_step and isf_counters_async first orders the
+ * handle's stream after that particle work; a caller that queues its own
+ * work on the handle's stream right after isf_step calls isf_join first.
+ * Work on the legacy default stream is ordered after both streams. */
 ISF_API int isf_get_stream(const isf_handle* h, void** stream);
 /* GPUArrays.synchronize (examples/benchmark.jl:66) */
 ISF_API int isf_sync(isf_handle* h);
+/* Order the handle's stream after the particle work of earlier isf_step
+ * calls (no host wait). */
+ISF_API int isf_join(isf_handle* h);
 /* Device buffers for psi / particles / masks (the reference's ArrayType(...) uploads, src/parallel.jl:78-97) */
 ISF_API int isf_malloc(isf_handle* h, void** dptr, size_t bytes);
 ISF_API int isf_free(isf_handle* h, void* dptr);

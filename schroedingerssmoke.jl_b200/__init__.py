@@ -44,7 +44,9 @@ class ISF:
     (src/parallel.jl:41-98): grid, d, velocity and the spectral tables live on
     the device of `device`."""
 
-    def __init__(self, physical_size, dims, hbar, dt, device: int = 0, flags: int = 0):
+    def __init__(self, physical_size, dims, hbar, dt, device: int = 0, flags: int = 0, stream=None):
+        # stream: a torch.cuda.Stream for all the handle's work (then without
+        # the separate particle stream), or None for a stream of its own
         if not torch.cuda.is_available():
             raise ISFError(_lib.ISF_ERR_CUDA, "no CUDA device: libisf has no CPU path")
         self.L = _lib.load()
@@ -55,7 +57,7 @@ class ISF:
         p.dt = float(dt)
         p.device = int(device)
         p.flags = int(flags)
-        p.stream = None
+        p.stream = None if stream is None else stream.cuda_stream
         h = C.c_void_p()
         check(self.L.isf_create(C.byref(p), C.byref(h)))
         self.h = h
@@ -89,6 +91,12 @@ class ISF:
     def sync(self):
         """GPUArrays.synchronize (examples/benchmark.jl:66)."""
         check(self.L.isf_sync(self.h), self.h)
+
+    def join(self):
+        """Order `self.stream` after the particle work (emission, advection)
+        that `step` leaves on the handle's particle stream; no host wait.
+        Every other call on the handle does this first."""
+        check(self.L.isf_join(self.h), self.h)
 
     @property
     def velocity(self) -> torch.Tensor:

@@ -18,7 +18,7 @@ EMIT_RING, EMIT_DISC, EMIT_CYLINDER = 0, 1, 2
 
 # every exported entry point of include/isf.h
 EXPORTS = (
-    "isf_create", "isf_destroy", "isf_last_error", "isf_get_stream", "isf_sync", "isf_malloc", "isf_free",
+    "isf_create", "isf_destroy", "isf_last_error", "isf_get_stream", "isf_sync", "isf_join", "isf_malloc", "isf_free",
     "isf_memcpy_h2d", "isf_memcpy_d2h", "isf_grid_info", "isf_schroedinger_flow", "isf_normalize_psi",
     "isf_pressure_project", "isf_velocity_one_form", "isf_staggered_sharp", "isf_get_velocity",
     "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
@@ -127,6 +127,7 @@ def load(path: str | None = None):
         "isf_create": [C.POINTER(IsfParams), C.POINTER(vp)],
         "isf_destroy": [vp],
         "isf_get_stream": [vp, C.POINTER(vp)],
+        "isf_join": [vp],
         "isf_sync": [vp],
         "isf_malloc": [vp, C.POINTER(vp), sz],
         "isf_free": [vp, vp],

@@ -139,7 +139,6 @@ bool check_params(const isf_params* p, std::string& why) {
 
 using namespace isf;
 
-
 namespace isf_int {
 
 thread_local std::string g_create_error;
@@ -175,26 +174,35 @@ cudaEvent_t prof_event(isf_handle* h) {
 }
 
 // Records an event pair around one launch when profiling is on.
-int prof_begin(isf_handle* h, const char* site) {
+int prof_begin(isf_handle* h, const char* site, cudaStream_t st) {
     if (!h->prof_on) return -1;
     isf_handle::Rec r;
     r.site = prof_site(h, site);
     r.a = prof_event(h);
     r.b = prof_event(h);
     if (!r.a || !r.b) return -1;
-    cudaEventRecord(r.a, h->stream);
+    cudaEventRecord(r.a, st ? st : h->stream);
     h->recs.push_back(r);
     return (int)h->recs.size() - 1;
 }
 
-void prof_end(isf_handle* h, int slot) {
-    if (slot >= 0) cudaEventRecord(h->recs[slot].b, h->stream);
+void prof_end(isf_handle* h, int slot, cudaStream_t st) {
+    if (slot >= 0) cudaEventRecord(h->recs[slot].b, st ? st : h->stream);
 }
 
+int join(isf_handle* h) {
+    if (!h->side_pending) return ISF_OK;
+    ISF_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_side, 0), "join the particle stream");
+    h->side_pending = false;
+    return ISF_OK;
+}
 
-
-
-
+void destroy_side(isf_handle* h) {
+    for (cudaEvent_t e : {h->ev_vel, h->ev_side, h->ev_read[0], h->ev_read[1]})
+        if (e) cudaEventDestroy(e);
+    if (h->side) cudaStreamDestroy(h->side);
+    h->side = nullptr;
+}
 
 XArgs xargs(isf_handle* h) {
     XArgs a;
@@ -246,8 +254,13 @@ StencilArgs stargs(isf_handle* h, const float* psi, float* out) {
     return a;
 }
 
-// velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the handle's velocity
+// velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the handle's
+// velocity: the plane set no in-flight advection reads, which becomes current
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site) {
+    const int nb = h->vcur ^ 1;
+    if (h->side) ISF_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_read[nb], 0), "velocity buffer reuse");
+    h->vcur = nb;
+    h->vel = h->vel_buf[nb];
     StencilArgs sa = stargs(h, psi, h->vel);
     sa.hbar = hbar;
     sa.sharp = sharp;
@@ -337,9 +350,11 @@ int isf_create(const isf_params* p, isf_handle** out) {
     auto cleanup = [&](int code, const std::string& msg) {
         if (h->F) cudaFree(h->F);
         if (h->f) cudaFree(h->f);
-        if (h->vel) cudaFree(h->vel);
+        for (float* v : h->vel_buf)
+            if (v) cudaFree(v);
         if (h->tables) cudaFree(h->tables);
         if (h->counters) cudaFree(h->counters);
+        destroy_side(h);
         if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
         delete h;
         return fail(nullptr, code, msg);
@@ -350,9 +365,17 @@ int isf_create(const isf_params* p, isf_handle** out) {
         e = cudaStreamCreateWithFlags(&h->stream, cudaStreamDefault);  // orders with the legacy default stream
         if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: stream: ") + cudaGetErrorString(e));
         h->own_stream = true;
+        // the particle stream of isf_step (blocking as well, so work on the
+        // legacy default stream is ordered after its advection)
+        e = cudaStreamCreateWithFlags(&h->side, cudaStreamDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_vel, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_side, cudaEventDisableTiming);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->ev_read[i], cudaEventDisableTiming);
+        if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: particle stream: ") + cudaGetErrorString(e));
     }
     if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess || cudaMalloc(&h->f, sizeof(float) * g.N) != cudaSuccess ||
-        cudaMalloc(&h->vel, sizeof(float) * 3 * g.NP) != cudaSuccess ||
+        cudaMalloc(&h->vel_buf[0], sizeof(float) * 3 * g.NP) != cudaSuccess ||
+        cudaMalloc(&h->vel_buf[1], sizeof(float) * 3 * g.NP) != cudaSuccess ||
         cudaMalloc(&h->tables, total) != cudaSuccess ||
         cudaMalloc(&h->counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
@@ -360,7 +383,8 @@ int isf_create(const isf_params* p, isf_handle** out) {
     }
     e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemset(h->vel, 0, sizeof(float) * 3 * g.NP);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemset(h->vel_buf[i], 0, sizeof(float) * 3 * g.NP);
+    h->vel = h->vel_buf[0];
     if (e == cudaSuccess) e = cudaMemset(h->F, 0, sizeof(float2) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
     bind_tables(g, reinterpret_cast<const char*>(h->tables));
@@ -373,12 +397,15 @@ int isf_destroy(isf_handle* h) {
     {
         DeviceGuard guard(h->device);
         if (h->stream) cudaStreamSynchronize(h->stream);
+        if (h->side) cudaStreamSynchronize(h->side);
         cudaFree(h->F);
         cudaFree(h->f);
-        cudaFree(h->vel);
+        cudaFree(h->vel_buf[0]);
+        cudaFree(h->vel_buf[1]);
         cudaFree(h->tables);
         cudaFree(h->counters);
         adj_free(h);
+        destroy_side(h);
         if (h->own_stream) cudaStreamDestroy(h->stream);
         for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     }
@@ -391,6 +418,11 @@ const char* isf_last_error(const isf_handle* h) { return h ? h->err.c_str() : g_
 int isf_sync(isf_handle* h) {
     ISF_ENTER(h);
     ISF_CUDA(h, cudaStreamSynchronize(h->stream), "isf_sync");
+    return ISF_OK;
+}
+
+int isf_join(isf_handle* h) {
+    ISF_ENTER(h);
     return ISF_OK;
 }
 
@@ -539,7 +571,7 @@ int isf_staggered_advect(isf_handle* h, float* parts, int64_t np) {
 }
 
 int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step_args* a) {
-    ISF_ENTER(h);
+    ISF_ENTER_NOJOIN(h);
     if (!psi || !a) return fail(h, ISF_ERR_INVALID, "isf_step: null argument");
     ISF_ALIGNED(h, psi, 16, "psi");
     if (np < 0 || (np > 0 && !parts)) return fail(h, ISF_ERR_INVALID, "isf_step: bad particles");
@@ -557,16 +589,6 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     rc = run_projection(h, psi, nullptr);     // pressure_project!
     if (rc) return rc;
     if (a->jet) {
-        if (a->emit_count > 0) {
-            EmitArgs e;
-            for (int k = 0; k < 3; ++k) e.cen[k] = a->nozzle_cen[k];
-            e.len = a->nozzle_len;
-            e.rad = a->nozzle_rad;
-            e.seed = a->seed;
-            e.counter = a->counter;
-            e.mode = a->emit_mode;
-            ISF_LAUNCH(h, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, h->stream), "step emit");
-        }
         JetArgs j = make_jet(a->kvec, a->jetmask, a->nozzle_cen, a->nozzle_len, a->nozzle_rad, a->omega_t,
                              a->phase_mode);
         rc = run_projection(h, psi, &j);  // restrict_velocity! + pressure_project!
@@ -575,8 +597,35 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     // velocity_one_form!(isf, psi, isf.hbar) + staggered sharp
     rc = run_one_form(h, psi, h->g.hbar, 1, "step one_form");
     if (rc) return rc;
-    if (np > 0) ISF_LAUNCH(h, launch_advect(h->g, parts, np, h->vel, h->counters, h->stream), "step advect");
+    // add_particles! (before the projections in the reference; the particles
+    // are independent of psi) and staggered_advect!.  With a particle stream
+    // they run there, after this step's velocity, while the caller queues the
+    // next step's psi passes; the velocity plane set they read is not written
+    // again until they are done (run_one_form alternates between two).
+    cudaStream_t ps = h->side ? h->side : h->stream;
+    const bool emit = a->jet && a->emit_count > 0;
+    if (h->side && (emit || np > 0)) {
+        ISF_CUDA(h, cudaEventRecord(h->ev_vel, h->stream), "step velocity event");
+        ISF_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_vel, 0), "step velocity event");
+    }
+    if (emit) {
+        EmitArgs e;
+        for (int k = 0; k < 3; ++k) e.cen[k] = a->nozzle_cen[k];
+        e.len = a->nozzle_len;
+        e.rad = a->nozzle_rad;
+        e.seed = a->seed;
+        e.counter = a->counter;
+        e.mode = a->emit_mode;
+        ISF_LAUNCH_ON(h, ps, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, ps), "step emit");
+    }
+    if (np > 0) ISF_LAUNCH_ON(h, ps, launch_advect(h->g, parts, np, h->vel, h->counters, ps), "step advect");
+    if (h->side && (emit || np > 0)) {
+        ISF_CUDA(h, cudaEventRecord(h->ev_read[h->vcur], h->side), "step particle event");
+        ISF_CUDA(h, cudaEventRecord(h->ev_side, h->side), "step particle event");
+        h->side_pending = true;
+    }
     if (h->flags & ISF_FLAG_CHECK_NAN) {
+        if (int rc_j = join(h)) return rc_j;  // after any counter reset queued on the particle stream
         // counters[15]: non-finite psi cells after this step
         ISF_CUDA(h, cudaMemsetAsync(h->counters + 15, 0, sizeof(unsigned long long), h->stream), "nan check");
         ISF_LAUNCH(h, launch_count_nonfinite(h->g, reinterpret_cast<const float4*>(psi), h->counters + 15, h->stream),
@@ -690,11 +739,16 @@ int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset) {
 }
 
 int isf_counters_async(isf_handle* h, uint64_t* host_out, int32_t n, int32_t reset) {
-    ISF_ENTER(h);
+    ISF_ENTER_NOJOIN(h);
     if (n < 1 || n > 16 || !host_out) return fail(h, ISF_ERR_INVALID, "isf_counters_async: n must be 1..16");
-    ISF_CUDA(h, cudaMemcpyAsync(host_out, h->counters, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, h->stream),
+    // behind the last step's advection on the particle stream, so the read
+    // does not hold the handle's stream back; everything else that touched
+    // the counters is ordered before that advection
+    cudaStream_t st = h->side_pending ? h->side : h->stream;
+    ISF_CUDA(h, cudaMemcpyAsync(host_out, h->counters, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, st),
              "counters");
-    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * 16, h->stream), "counters reset");
+    if (reset) ISF_CUDA(h, cudaMemsetAsync(h->counters, 0, sizeof(unsigned long long) * 16, st), "counters reset");
+    if (h->side_pending) ISF_CUDA(h, cudaEventRecord(h->ev_side, h->side), "counters event");
     return ISF_OK;
 }
 

@@ -427,6 +427,7 @@ int isf_adj_loss(isf_handle* h, const isf_adj_problem* p, const float* psi0, con
     for (int n = 1; n <= p->nsteps; ++n) {
         isf_step_args st = problem_step(p, h->g.dt, n, nullptr);
         if (int rc = isf_step(h, reinterpret_cast<float*>(work), a->positions, np, &st)) return rc;
+        if (int rc = join(h)) return rc;  // the step's particles, on the handle's stream
     }
     if (int rc = clear_acc(h)) return rc;
     ISF_LAUNCH(h, launch_loss(a->positions, targets, a->lam, np, a->acc + 4, h->stream), "adj loss");
@@ -478,6 +479,7 @@ int isf_adj_gradient(isf_handle* h, const isf_adj_problem* p, const float* psi0,
             if (int rc = copy_psi(h, ckpt + ((n - 1) / K) * N, work)) return rc;
         if (n < last0) {
             if (int rc = isf_step(h, reinterpret_cast<float*>(work), cur, np, &st)) return rc;
+            if (int rc = join(h)) return rc;  // the step's particles, on the handle's stream
         } else {
             const StepJet sj = step_jet(&st);
             const float4* out = nullptr;

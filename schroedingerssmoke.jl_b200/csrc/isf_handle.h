@@ -20,7 +20,16 @@ struct isf_handle {
     int flags = 0;           // ISF_FLAG_* of isf_create
     int kmajor = 0;          // the half spectrum is k-major and solved plane by plane (plane_supported)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
-    float* vel = nullptr;    // padded velocity planes vx | vy | vz, 3 NP
+    float* vel = nullptr;    // the current padded velocity planes vx | vy | vz (3 NP): vel_buf[vcur]
+    float* vel_buf[2] = {nullptr, nullptr};  // two plane sets: a step writes one while the
+    int vcur = 0;                            // previous step's advection may still read the other
+    // isf_step runs its particle work (emission, advection) on `side`, so the
+    // next step's psi passes overlap it; only for handles that own their stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_vel = nullptr;              // the step's velocity is written (main stream)
+    cudaEvent_t ev_read[2] = {nullptr, nullptr};  // the advection that read vel_buf[i] is done (side)
+    cudaEvent_t ev_side = nullptr;             // the last work queued on side
+    bool side_pending = false;                 // side work the main stream has not waited for
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
     unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
     unsigned long long launches = 0;         // kernels launched by this handle
@@ -46,8 +55,10 @@ using namespace isf;
 
 int fail(isf_handle* h, int code, const std::string& msg);
 int cuda_fail(isf_handle* h, cudaError_t e, const char* where);
-int prof_begin(isf_handle* h, const char* site);
-void prof_end(isf_handle* h, int slot);
+int prof_begin(isf_handle* h, const char* site, cudaStream_t st = nullptr);
+void prof_end(isf_handle* h, int slot, cudaStream_t st = nullptr);
+// make the main stream wait for the particle work isf_step queued on the side stream
+int join(isf_handle* h);
 
 // Make the handle's device current for the duration of a call.
 struct DeviceGuard {
@@ -111,7 +122,24 @@ void adj_free(isf_handle* h);
             return fail(h, ISF_ERR_INVALID, std::string(name) + " must be " #a "-byte aligned"); \
     } while (0)
 
-#define ISF_ENTER(h)                                          \
+// Every entry point except isf_step and isf_counters_async first orders the
+// handle's stream after the particle work earlier steps left on the side
+// stream, so it sees their particles, counters and velocity reads finished.
+#define ISF_ENTER_NOJOIN(h)                                   \
     ISF_CHECK_HANDLE(h);                                      \
     DeviceGuard guard_(h->device);                            \
     if (guard_.err != cudaSuccess) return cuda_fail(h, guard_.err, "cudaSetDevice")
+
+#define ISF_ENTER(h)                                          \
+    ISF_ENTER_NOJOIN(h);                                      \
+    if (int rc_join_ = join(h)) return rc_join_
+
+// a launch on another stream than the handle's (profiling events on it)
+#define ISF_LAUNCH_ON(h, st, expr, site)                         \
+    do {                                                         \
+        const int ps_ = prof_begin(h, site, st);                 \
+        cudaError_t e_ = (expr);                                 \
+        ++(h)->launches;                                         \
+        prof_end(h, ps_, st);                                    \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, site);    \
+    } while (0)

@@ -222,12 +222,16 @@ cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, i
     return launch_pdl(k_emit, grid, dim3(blk), 0, s, parts, nslots, 0LL, count, EmitArgs{}, emits);
 }
 
+#ifndef ISF_ADVECT_WAVES
+#define ISF_ADVECT_WAVES 1
+#endif
+
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel, unsigned long long* counters,
                           cudaStream_t s, int nsim, long long bs_vel) {
     if (np <= 0 || nsim <= 0) return cudaSuccess;
     if (np > kMaxParticles) return cudaErrorInvalidValue;
     const int blk = 256;
-    // one resident wave, grid-stride over the slots
+    // ISF_ADVECT_WAVES resident waves (0: one CTA per 256 slots), grid-stride over the slots
     static int resident = 0;  // CTAs per SM of either instantiation (the same registers)
     if (resident == 0) {
         int dev = 0, sms = 0, per = 0;
@@ -238,7 +242,7 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
         resident = sms * per;
     }
     long long b = (np + blk - 1) / blk;
-    if (b > resident) b = resident;
+    if (ISF_ADVECT_WAVES > 0 && b > (long long)ISF_ADVECT_WAVES * resident) b = (long long)ISF_ADVECT_WAVES * resident;
     const dim3 grid((unsigned)b, (unsigned)nsim);
     const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
     if (g.norm_w)

@@ -316,3 +316,56 @@ def test_step_nan_check(isfpkg):
     assert e.value.code == 4
     with pytest.raises(isfpkg.ISFError, match="unknown flags"):
         isfpkg.ISF(L, dims, HBAR, DT, flags=64)
+
+
+def test_particle_stream_matches_single_stream(isfpkg, cfgs):
+    """A handle that owns its stream runs the particle work of isf_step on a
+    second stream, overlapped with the next step's psi passes, and alternates
+    two velocity plane sets; a handle on a caller stream runs everything in
+    order on that stream.  Both give the same bits: psi, particles, velocity and
+    the per-step counters read with isf_counters_async."""
+    L, dims = (4, 2, 2), (64, 32, 32)
+    noz = cfgs.JET_NOZZLE
+    kvec, omega = cfgs.jet_omega()
+    rng = np.random.default_rng(21)
+    psi0 = cuda(cfgs.jet_init_psi(dims))
+    P = 30000
+    p0 = rng.uniform(0, 1, (P, 3)) * np.asarray(L)
+    p0[:10000] = -1.0  # slots the jet fills
+    parts0 = cuda(p0)
+    caller = torch.cuda.Stream()
+    two = isfpkg.ISF(L, dims, HBAR, DT)
+    one = isfpkg.ISF(L, dims, HBAR, DT, stream=caller)
+    steps = 12
+    res = {}
+    out = {}
+    torch.cuda.synchronize()
+    for name, isf in (("two", two), ("one", one)):
+        psi, parts = psi0.clone(), parts0.clone()
+        torch.cuda.synchronize()
+        rows = torch.zeros((steps, 2), dtype=torch.int64).pin_memory()
+        for it in range(1, steps + 1):
+            jet = dict(kvec=kvec, omega_t=float(np.float32(omega) * np.float32(it * np.float32(DT))),
+                       cen=noz["cen"], len=noz["len"], rad=noz["rad"], emit_start=(it * 800) % 10000,
+                       emit_count=800, seed=5, counter=it, emit_mode=1, phase_mode=1)
+            isfpkg.step(isf, psi, parts, jet if it % 3 else None)
+            isf.counters_async(rows[it - 1], reset=True)
+        if name == "two":
+            # work queued on the handle's stream after isf_join sees the advection
+            isf.join()
+            with torch.cuda.stream(isf.stream):
+                snap = parts.clone()
+            isf.sync()
+            out["snap"] = snap
+        else:
+            isf.sync()
+        res[name] = rows.clone()
+        out[name] = (psi, parts, isf.velocity)
+    psi_a, parts_a, vel_a = out["two"]
+    psi_b, parts_b, vel_b = out["one"]
+    assert torch.equal(psi_a, psi_b)
+    assert torch.equal(parts_a, parts_b)
+    assert torch.equal(out["snap"], parts_b)
+    assert torch.equal(vel_a, vel_b)
+    assert torch.equal(res["two"], res["one"])
+    assert int(res["two"][-1, 1]) > 20000
