@@ -304,6 +304,38 @@ def batched_vs_plain(pkg, cfgs, steps, warmup, local):
             "ms_per_ensemble_step": t_batch / steps, "classes": ncls, "tiles": tiles}
 
 
+def sharded_ensemble(pkg, cfgs, steps, warmup, rank, world, local):
+    """The C4 ensemble spread over the ranks: each rank steps its share of the
+    64 jets (configs.shard, balanced by bytes per step) as one batch on its own
+    GPU, with no collective on the data path.  Timed with CUDA events on each
+    batch's stream; the whole job's rate uses the slowest rank."""
+    import torch
+    sims, psi0, parts0 = cfgs.ensemble(nsims=64, seed=3, nslots=65536)
+    mine = cfgs.shard([cfgs.sim_cost(s) for s in sims], world)[rank]
+    dev = f"cuda:{local}"
+    b = pkg.ISFBatch([sims[i] for i in mine], device=local, tune=True)
+    for k, i in enumerate(mine):
+        b.set_psi(k, torch.from_numpy(psi0[i]).to(dev))
+        b.set_particles(k, torch.from_numpy(parts0[i]).to(dev))
+    b.init_jet(10)
+    b.step(warmup)
+    b.sync()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(b.stream)
+    b.step(steps)
+    e1.record(b.stream)
+    e1.synchronize()
+    ms = rank_max(e0.elapsed_time(e1), world, dev)
+    b.close()
+    return {"workload": "ensemble_64_jets_32^3-96x48x48_65536_particles", "sims": len(sims), "ranks": world,
+            "sims_this_rank": len(mine), "steps": steps, "sim_steps_per_s": len(sims) * steps / (ms / 1000.0),
+            "what": "the 64 simulations split over the ranks by bytes per step, one batch per GPU, "
+                    "max over ranks"}
+
+
 def adjoint_vs_forward(pkg, cfgs, reps, local):
     """The particle-loss gradient of the 64x32x32 jet (65 536 particles
     uniform in the box, 10 initialisation projections, 50 steps, psi
@@ -463,6 +495,9 @@ def main():
                "what": "isf_memcpy_h2d of psi0 + particles, K x (isf_step + 16-byte counter read into pinned "
                        "host memory, isf_counters_async), isf_memcpy_d2h of psi + particles",
                "live_particles_last_step": live}
+    sharded = None
+    if world > 1 and not args.no_batch:
+        sharded = sharded_ensemble(pkg, cfgs, min(args.steps, 100), args.warmup, rank, world, local)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -495,7 +530,7 @@ def main():
                           "unit": "GB/s", "frac": step_achieved / peak},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
-        "batched": batched, "adjoint": adjoint,
+        "batched": batched, "batched_sharded": sharded, "adjoint": adjoint,
     }
     print(json.dumps(line), flush=True)
 

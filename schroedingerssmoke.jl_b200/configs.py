@@ -178,3 +178,28 @@ def ensemble(nsims=64, seed=3, nslots=65536, hbar=HBAR, dt=float(np.float32(1 / 
         p = nozzle_particles(nslots, noz["cen"], noz["len"], noz["rad"], seed * 1000 + i)
         parts0.append(p[cell_sort_order(p, L, dims)].astype(np.float32))
     return sims, psi0, parts0
+
+
+def sim_cost(sim) -> int:
+    """Bytes one no-jet step of a simulation moves by the per-step convention
+    of the step roofline: 196 B per cell + 24 B per particle slot (a jet step
+    adds 76 B per cell on every simulation alike, so the ranking is the same)."""
+    n = sim["dims"]
+    return 196 * int(n[0]) * int(n[1]) * int(n[2]) + 24 * int(sim.get("nslots", 0))
+
+
+def shard(costs, world: int):
+    """Split independent simulations over `world` ranks (one GPU each, no
+    collective): longest first onto the least loaded rank, ties to the lower
+    rank and the lower index, so every rank computes the same split.  Returns
+    one ascending index list per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += costs[i]
+        parts[r].append(i)
+    return [sorted(p) for p in parts]
