@@ -101,6 +101,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
+    ap.add_argument("--no-matlabport", action="store_true", help="skip the MatlabPort front-end loop")
     return ap.parse_args()
 
 
@@ -336,6 +337,92 @@ def sharded_ensemble(pkg, cfgs, steps, warmup, rank, world, local):
                     "max over ranks"}
 
 
+MATLAB_CFG = dict(L=(4, 2, 2), dims=(64, 32, 32), hbar=0.1, dt=1 / 48, slots=20000, births=10)
+
+
+def matlabport_loop(pkg, cfgs, steps, warmup, local):
+    """The MatlabPort driver loop (examples/matlabport/simple.jl:20-124) on the
+    64x32x32 jet through the FP64 structure-of-arrays front-end: FP64 psi1,
+    psi2 and velocity arrays between the calls, 20 000 particle slots, 10
+    births per step, removethedead! every step.  Device-timed with CUDA events
+    on the legacy default stream, which the library's blocking streams are
+    ordered with."""
+    import torch
+    mp = pkg.matlabport
+    c = MATLAB_CFG
+    L, dims, hbar, dt = c["L"], c["dims"], c["hbar"], c["dt"]
+    noz = cfgs.JET_NOZZLE
+    vjet = np.array([1.0, 0.0, 0.0])
+    kvec, omega = vjet / hbar, float(np.sum(vjet ** 2) / (2 * hbar))
+    obj = mp.ISF(L, dims, hbar, dt, device=local)
+    isjet = mp.is_jet(obj, noz["cen"], noz["len"], noz["rad"])
+    dev = f"cuda:{local}"
+    a1, a2 = mp.Normalize(torch.ones(dims, dtype=torch.complex128, device=dev),
+                          0.01 * torch.ones(dims, dtype=torch.complex128, device=dev))
+    for _ in range(10):
+        a1, a2 = mp.restrict(obj, a1, a2, isjet, kvec, 0.0)
+        a1, a2 = mp.PressureProject(obj, a1, a2)
+    slots, nb = c["slots"], c["births"]
+    p = mp.Particles(np.zeros(slots), np.zeros(slots), np.zeros(slots), device=local)
+
+    def body(it, a1, a2):
+        t = it * dt
+        a1, a2 = mp.SchroedingerFlow(obj, a1, a2)
+        a1, a2 = mp.Normalize(a1, a2)
+        a1, a2 = mp.PressureProject(obj, a1, a2)
+        a1, a2 = mp.restrict(obj, a1, a2, isjet, kvec, omega * t)
+        a1, a2 = mp.PressureProject(obj, a1, a2)
+        mp.add_ring(p, nb, noz["cen"], noz["rad"], seed=0, counter=it)
+        mp.remove_dead(p, obj)
+        vx, vy, vz = mp.VelocityOneForm(obj, a1, a2, obj.hbar)
+        vx, vy, vz = mp.StaggeredSharp(obj, vx, vy, vz)
+        mp.StaggeredAdvect(p, obj, vx, vy, vz, obj.dt)
+        return a1, a2
+
+    steps = min(steps, (slots - 1) // nb - warmup - 1)
+    for it in range(1, warmup + 1):
+        a1, a2 = body(it, a1, a2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for it in range(warmup + 1, warmup + steps + 1):
+        a1, a2 = body(it, a1, a2)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"workload": "matlabport_driver_jet_64x32x32_20000_slots_10_births_per_step", "steps": steps,
+            "steps_per_s": 1000.0 / ms, "ms_per_step": ms, "live_particles": int(p.active.numel()),
+            "what": "SchroedingerFlow, Normalize, PressureProject, restrict, PressureProject, add_ring, "
+                    "remove_dead (one host read of the live count), VelocityOneForm, StaggeredSharp, "
+                    "StaggeredAdvect on FP64 arrays"}
+
+
+def matlabport_cpu_baseline(cfgs, k=3):
+    """The same driver loop in the FP64 numpy restatement of MatlabPort.jl
+    (oracle/matlabport.py) on the host, k steps: steps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import matlabport as orc_mp
+    c = MATLAB_CFG
+    noz = cfgs.JET_NOZZLE
+    vjet = np.array([1.0, 0.0, 0.0])
+    kvec, omega = vjet / c["hbar"], float(np.sum(vjet ** 2) / (2 * c["hbar"]))
+    oo = orc_mp.MatlabISF(c["L"], c["dims"], c["hbar"], c["dt"])
+    isjet = orc_mp.is_jet(oo, noz["cen"], noz["len"], noz["rad"])
+    b1, b2 = orc_mp.normalize(np.ones(c["dims"], np.complex128), 0.01 * np.ones(c["dims"], np.complex128))
+    x, y, z = (np.zeros(c["slots"], np.float32) for _ in range(3))
+    n, act = 0, np.zeros(0, np.int64)
+    rng = np.random.default_rng(0)
+    t0 = time.perf_counter()
+    for it in range(1, k + 1):
+        th = rng.uniform(0, 2 * np.pi, c["births"]).astype(np.float32)
+        births = (np.full(c["births"], noz["cen"][0], np.float32),
+                  (noz["cen"][1] + 0.9 * noz["rad"] * np.cos(th)).astype(np.float32),
+                  (noz["cen"][2] + 0.9 * noz["rad"] * np.sin(th)).astype(np.float32))
+        b1, b2, n, act = orc_mp.driver_step(oo, b1, b2, isjet, kvec, omega * it * c["dt"], x, y, z, n, act, births)
+    return {"value": k / (time.perf_counter() - t0), "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"{k} steps of the same loop in numpy FP64"}
+
+
 def adjoint_vs_forward(pkg, cfgs, reps, local):
     """The particle-loss gradient of the 64x32x32 jet (65 536 particles
     uniform in the box, 10 initialisation projections, 50 steps, psi
@@ -509,10 +596,15 @@ def main():
     adjoint = None
     if not args.no_adjoint:
         adjoint = adjoint_vs_forward(pkg, cfgs, 3, local)
+    matlab = None
+    if not args.no_matlabport:
+        matlab = matlabport_loop(pkg, cfgs, min(args.steps, 200), args.warmup, local)
 
     cb = None
     if not args.no_cpu:
         cb = cpu_baseline(c, psi0, parts0, args.cpu_seconds)
+        if matlab is not None:
+            matlab["cpu_baseline"] = matlabport_cpu_baseline(cfgs)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -530,7 +622,7 @@ def main():
                           "unit": "GB/s", "frac": step_achieved / peak},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
-        "batched": batched, "batched_sharded": sharded, "adjoint": adjoint,
+        "batched": batched, "batched_sharded": sharded, "adjoint": adjoint, "matlabport": matlab,
     }
     print(json.dumps(line), flush=True)
 

@@ -61,8 +61,10 @@ enum {
  * or the dot product k . x (examples/matlabport/simple.jl:47,107) */
 enum { ISF_PHASE_REFERENCE_SUM = 0, ISF_PHASE_DOT = 1 };
 
-/* emission: reference ring (src/particles.jl:86-90), nozzle disc, nozzle cylinder */
-enum { ISF_EMIT_RING = 0, ISF_EMIT_DISC = 1, ISF_EMIT_CYLINDER = 2 };
+/* emission: reference ring (src/particles.jl:86-90), nozzle disc, nozzle
+ * cylinder, and the MatlabPort driver's ring of 0.9 r in the plane x = cen.x
+ * without jitter (examples/matlabport/simple.jl:112-115) */
+enum { ISF_EMIT_RING = 0, ISF_EMIT_DISC = 1, ISF_EMIT_CYLINDER = 2, ISF_EMIT_RING_PLANE = 3 };
 
 typedef struct isf_handle isf_handle;
 
@@ -346,6 +348,60 @@ ISF_API int isf_profile_get(const isf_handle* h, int32_t i, char* name, size_t c
                             int64_t* launches);
 /* kernels launched by h since isf_create */
 ISF_API int isf_launch_count(const isf_handle* h, uint64_t* out);
+
+/* ---- FP64 structure-of-arrays front-end (src/MatlabPort.jl)
+ *
+ * MatlabPort.jl is the reference's second formulation of the same operators
+ * (MatlabPort.jl:38-273): separate Complex{Float64} arrays psi1 and psi2,
+ * Float64 velocity components vx, vy, vz and scalar fields, all column-major
+ * with x fastest, and a Particles type holding Float32 x, y, z vectors and a
+ * list of active slots.  These entry points convert between that layout and
+ * the handle's FP32 layouts on the device, so the MatlabPort API runs on the
+ * kernels above (FP32 arithmetic inside).  Complex128 arrays are interleaved
+ * (re, im) and 16-byte aligned; slot lists are int64, 0-based, at most
+ * 2^31 - 1 long, and their slots distinct.  A slot outside [0, nslots) is
+ * skipped and counted in counter [12] (isf_counters). */
+
+/* psi (float4 per cell) from / to psi1, psi2 (complex128 per cell) */
+ISF_API int isf_psi_from_f64(isf_handle* h, const double* psi1, const double* psi2, float* psi);
+ISF_API int isf_psi_to_f64(isf_handle* h, const float* psi, double* psi1, double* psi2);
+/* the handle's velocity from / to vx, vy, vz (float64 per cell) */
+ISF_API int isf_velocity_from_f64(isf_handle* h, const double* vx, const double* vy, const double* vz);
+ISF_API int isf_velocity_to_f64(isf_handle* h, double* vx, double* vy, double* vz);
+/* dst[i] = (float)(scale * src[i * stride]), i < n: a real field, or the real
+ * (src) or imaginary (src + 1) part of a complex128 array with stride 2 */
+ISF_API int isf_real_from_f64(isf_handle* h, const double* src, int64_t stride, double scale, float* dst, int64_t n);
+/* dst[i] = (double)src[i], i < n */
+ISF_API int isf_real_to_f64(isf_handle* h, const float* src, double* dst, int64_t n);
+/* dst[i] = re[i] + i im[i] as complex128, i < n (im may be NULL: 0) */
+ISF_API int isf_complex_to_f64(isf_handle* h, const float* re, const float* im, double* dst, int64_t n);
+/* psi .= gauge_transform.(psi, q) with complex q = q_re + i q_im (q_im may be
+ * NULL): psi * exp(-i q) per cell        src/parallel.jl:125-129
+ * (GaugeTransform of MatlabPort.jl:139-144 multiplies by exp(+i q): pass -q) */
+ISF_API int isf_gauge_transform(isf_handle* h, float* psi, const float* q_re, const float* q_im);
+/* isf_add_particles into x, y, z vectors (the slots of a Particles) */
+ISF_API int isf_add_particles_soa(isf_handle* h, float* x, float* y, float* z, int64_t nslots, int64_t start,
+                                  int64_t count, const float cen[3], float len, float rad, uint64_t seed,
+                                  uint64_t counter, int32_t mode);
+/* StaggeredVelocity(px, py, pz, torus, vx, vy, vz) at n points on the
+ * handle's velocity                       src/MatlabPort.jl:238-273 */
+ISF_API int isf_staggered_velocity(isf_handle* h, const float* x, const float* y, const float* z, int64_t n,
+                                   float* ux, float* uy, float* uz);
+/* StaggeredAdvect(p, torus, vx, vy, vz, dt) on the handle's velocity: RK4
+ * for the slots active[0..n) (NULL: slots 0..n-1) with no box test; points
+ * wrap by mod inside the interpolation only   src/MatlabPort.jl:200-222 */
+ISF_API int isf_advect_active(isf_handle* h, float* x, float* y, float* z, int64_t nslots, const int64_t* active,
+                              int64_t n, float dt);
+/* removethedead! (examples/matlabport/simple.jl:67-74): the slots of
+ * active[0..n) (NULL: 0..n-1) whose position is strictly inside the box, in
+ * order, into out_active; their number into *out_n, a device int64.
+ * out_active must not overlap active. */
+ISF_API int isf_keep_inside(isf_handle* h, const float* x, const float* y, const float* z, int64_t nslots,
+                            const int64_t* active, int64_t n, int64_t* out_active, int64_t* out_n);
+/* Keep(particle, ind): ox[i] = x[ind[i]] etc., i < n   src/MatlabPort.jl:228-233
+ * (a slot outside [0, nslots) gives -1) */
+ISF_API int isf_gather_particles(isf_handle* h, const float* x, const float* y, const float* z, int64_t nslots,
+                                 const int64_t* ind, int64_t n, float* ox, float* oy, float* oz);
 
 #ifdef __cplusplus
 }

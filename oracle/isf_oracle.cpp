@@ -513,6 +513,8 @@ struct Orc {
 // mode 1: uniform in the nozzle cross-section disc at x = cen.x (MatlabPort driver
 //         spawns at the nozzle centre plane, examples/matlabport/simple.jl:115-118)
 // mode 2: uniform in the nozzle cylinder volume
+// mode 3: the MatlabPort driver's ring: 0.9 r in the plane x = cen.x, no jitter
+//         (examples/matlabport/simple.jl:112-115)
 // Stream: counter = (j, counter_lo, counter_hi, 0x15F0015F), key = (seed_lo, seed_hi).
 template <class R>
 void emit(R* parts, long nslots, long start, long count, const float cen[3], float len, float rad, uint64_t seed,
@@ -522,7 +524,12 @@ void emit(R* parts, long nslots, long start, long count, const float cen[3], flo
         orc_u32x4 r = orc_philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
         const float u0 = orc_u01(r.v[0]), u1 = orc_u01(r.v[1]), u2 = orc_u01(r.v[2]), u3 = orc_u01(r.v[3]);
         R p[3];
-        if (mode == 0) {
+        if (mode == 3) {
+            const R rt = (R)u0 * (R)2 * (R)kPi;
+            p[0] = (R)cen[0];
+            p[1] = (R)cen[1] + (R)0.9f * (R)rad * std::cos(rt);
+            p[2] = (R)cen[2] + (R)0.9f * (R)rad * std::sin(rt);
+        } else if (mode == 0) {
             const R rt = (R)u0 * (R)2 * (R)kPi;
             const R o0 = (R)u1 * (R)0.1f - (R)0.05f, o1 = (R)u2 * (R)0.1f - (R)0.05f, o2 = (R)u3 * (R)0.1f - (R)0.05f;
             p[0] = ((R)cen[0] - (R)0.1f) + o0;

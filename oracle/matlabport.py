@@ -182,6 +182,46 @@ def jet_step(obj, psi1, psi2, isjet, kvec, omega_t, parts=None):
     return psi1, psi2, parts
 
 
+def driver_step(obj, psi1, psi2, isjet, kvec, omega_t, x, y, z, length, active, births):
+    """One iteration of the MatlabPort driver loop (examples/matlabport/simple.jl:99-124)
+    with its Particles semantics: the births (bx, by, bz) fill the slots after
+    `length` and become active (append!, MatlabPort.jl:186-196), removethedead!
+    keeps the active slots strictly inside the box in order, and
+    StaggeredAdvect moves the active slots with no box test
+    (MatlabPort.jl:200-222).  x, y, z are float32 slot vectors, updated in
+    place; returns (psi1, psi2, length, active)."""
+    psi1, psi2 = schroedinger_flow(obj, psi1, psi2)
+    psi1, psi2 = normalize(psi1, psi2)
+    psi1, psi2 = pressure_project(obj, psi1, psi2)
+    psi1, psi2 = restrict(obj, psi1, psi2, isjet, kvec, omega_t)
+    psi1, psi2 = pressure_project(obj, psi1, psi2)
+    bx, by, bz = births
+    n = len(bx)
+    assert n + length < len(x)
+    x[length:length + n], y[length:length + n], z[length:length + n] = bx, by, bz
+    active = np.concatenate([np.asarray(active, np.int64), np.arange(length, length + n, dtype=np.int64)])
+    length += n
+    keep = inside(obj, x[active], y[active], z[active])
+    active = active[keep]
+    vx, vy, vz = velocity_one_form(obj, psi1, psi2, obj.hbar)
+    vx, vy, vz = staggered_sharp(obj, vx, vy, vz)
+    px, py, pz = (v[active].astype(np.float64) for v in (x, y, z))
+    nx, ny, nz = staggered_advect(px, py, pz, obj, vx, vy, vz, obj.dt)
+    x[active], y[active], z[active] = nx, ny, nz
+    return psi1, psi2, length, active
+
+
+def face_margin(obj, px, py, pz):
+    """Distance of each point (after mod) to the nearest cell face in units of
+    the cell, min over the axes: where it is tiny, an FP32 and an FP64
+    evaluation may pick different cells."""
+    m = np.full(np.shape(px), np.inf)
+    for p, L, d in ((px, obj.sizex, obj.dx), (py, obj.sizey, obj.dy), (pz, obj.sizez, obj.dz)):
+        q = np.mod(np.asarray(p, np.float64), L) / d
+        m = np.minimum(m, np.abs(q - np.round(q)))
+    return m
+
+
 # ---- layout helpers between [x,y,z] component arrays and the oracle's
 # (nz, ny, nx, 4) AoS psi
 def to_aos(psi1, psi2):

@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 SOURCES = [os.path.join(HERE, "isf_oracle.cpp"), os.path.join(HERE, "philox.h")]
 
 # emission modes (particles.jl:86-90 ring / nozzle disc / nozzle cylinder)
-EMIT_RING, EMIT_DISC, EMIT_CYLINDER = 0, 1, 2
+EMIT_RING, EMIT_DISC, EMIT_CYLINDER, EMIT_RING_PLANE = 0, 1, 2, 3
 # jet phase modes: reference tuple_dot = sum(k .+ x) (particles.jl:1,15) / k.x
 PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
 

@@ -20,13 +20,13 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
                    PHASE_REFERENCE_SUM, IsfParams, IsfStepArgs, ISFError, check, f3)
 
 __all__ = [
     "ISF", "ISFBatch", "ISFError", "ParticleLoss", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
     "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
-    "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER", "FLAG_NORMALIZED_WEIGHTS",
+    "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER", "EMIT_RING_PLANE", "FLAG_NORMALIZED_WEIGHTS",
     "FLAG_CHECK_NAN",
 ]
 
@@ -564,3 +564,6 @@ class ParticleLoss(torch.autograd.Function):
         gk = torch.tensor(ctx.jb[:3], dtype=torch.float32, device=gpsi.device) * g
         gw = torch.tensor(ctx.jb[3], dtype=torch.float32, device=gpsi.device) * g
         return gpsi * g, gk, gw, None, None, None, None
+
+
+from . import matlabport  # noqa: E402  (the FP64 structure-of-arrays front-end)

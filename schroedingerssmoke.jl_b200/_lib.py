@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libisf.so")
 ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM, ISF_ERR_NAN = 0, 1, 2, 3, 4
 FLAG_NORMALIZED_WEIGHTS, FLAG_CHECK_NAN = 1, 2
 PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
-EMIT_RING, EMIT_DISC, EMIT_CYLINDER = 0, 1, 2
+EMIT_RING, EMIT_DISC, EMIT_CYLINDER, EMIT_RING_PLANE = 0, 1, 2, 3
 
 # every exported entry point of include/isf.h
 EXPORTS = (
@@ -31,6 +31,9 @@ EXPORTS = (
     "isf_adj_schroedinger_flow", "isf_adj_normalize_psi", "isf_adj_pressure_project", "isf_adj_restrict_velocity",
     "isf_adj_velocity_one_form", "isf_adj_staggered_advect", "isf_adj_get_velocity_bar", "isf_adj_set_velocity_bar",
     "isf_adj_step", "isf_adj_loss", "isf_adj_gradient",
+    "isf_psi_from_f64", "isf_psi_to_f64", "isf_velocity_from_f64", "isf_velocity_to_f64", "isf_real_from_f64",
+    "isf_real_to_f64", "isf_complex_to_f64", "isf_gauge_transform", "isf_add_particles_soa",
+    "isf_staggered_velocity", "isf_advect_active", "isf_keep_inside", "isf_gather_particles",
 )
 TILE_KINDS = ("x_psi", "x_real", "y_psi", "z_psi", "y_half", "z_half")
 
@@ -183,6 +186,19 @@ def load(path: str | None = None):
         "isf_adj_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs), vp, vp, dp],
         "isf_adj_loss": [vp, C.POINTER(IsfAdjProblem), vp, vp, i64, vp, dp],
         "isf_adj_gradient": [vp, C.POINTER(IsfAdjProblem), vp, vp, i64, vp, dp, vp, vp, dp],
+        "isf_psi_from_f64": [vp, vp, vp, vp],
+        "isf_psi_to_f64": [vp, vp, vp, vp],
+        "isf_velocity_from_f64": [vp, vp, vp, vp],
+        "isf_velocity_to_f64": [vp, vp, vp, vp],
+        "isf_real_from_f64": [vp, vp, i64, C.c_double, vp, i64],
+        "isf_real_to_f64": [vp, vp, vp, i64],
+        "isf_complex_to_f64": [vp, vp, vp, vp, i64],
+        "isf_gauge_transform": [vp, vp, vp, vp],
+        "isf_add_particles_soa": [vp, vp, vp, vp, i64, i64, i64, fp, f32, f32, u64, u64, i32],
+        "isf_staggered_velocity": [vp, vp, vp, vp, i64, vp, vp, vp],
+        "isf_advect_active": [vp, vp, vp, vp, i64, vp, i64, f32],
+        "isf_keep_inside": [vp, vp, vp, vp, i64, vp, i64, vp, vp],
+        "isf_gather_particles": [vp, vp, vp, vp, i64, vp, i64, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -404,6 +404,7 @@ int isf_destroy(isf_handle* h) {
         cudaFree(h->vel_buf[1]);
         cudaFree(h->tables);
         cudaFree(h->counters);
+        cudaFree(h->keep_counts);
         adj_free(h);
         destroy_side(h);
         if (h->own_stream) cudaStreamDestroy(h->stream);
@@ -550,7 +551,7 @@ int isf_add_particles(isf_handle* h, float* parts, int64_t nslots, int64_t start
     if (!parts || !cen) return fail(h, ISF_ERR_INVALID, "isf_add_particles: null argument");
     if (nslots <= 0 || count < 0 || start < 0) return fail(h, ISF_ERR_INVALID, "isf_add_particles: bad slot range");
     if (count > nslots) return fail(h, ISF_ERR_INVALID, "isf_add_particles: count exceeds the number of slots");
-    if (mode < ISF_EMIT_RING || mode > ISF_EMIT_CYLINDER) return fail(h, ISF_ERR_INVALID, "isf_add_particles: bad mode");
+    if (mode < ISF_EMIT_RING || mode > ISF_EMIT_RING_PLANE) return fail(h, ISF_ERR_INVALID, "isf_add_particles: bad mode");
     EmitArgs e;
     for (int a = 0; a < 3; ++a) e.cen[a] = cen[a];
     e.len = len;
@@ -581,7 +582,7 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
             return fail(h, ISF_ERR_INVALID, "isf_step: bad phase_mode");
         if (a->emit_count < 0 || a->emit_start < 0 || (a->emit_count > 0 && (np <= 0 || a->emit_count > np)))
             return fail(h, ISF_ERR_INVALID, "isf_step: bad emission range");
-        if (a->emit_count > 0 && (a->emit_mode < ISF_EMIT_RING || a->emit_mode > ISF_EMIT_CYLINDER))
+        if (a->emit_count > 0 && (a->emit_mode < ISF_EMIT_RING || a->emit_mode > ISF_EMIT_RING_PLANE))
             return fail(h, ISF_ERR_INVALID, "isf_step: bad emit_mode");
     }
     int rc = run_schroedinger(h, psi, true);  // schroedinger_flow! + normalize_psi

@@ -433,7 +433,7 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
                 return bfail(nullptr, ISF_ERR_INVALID, who + "bad phase_mode");
             if (d.emit_per_step < 0 || d.emit_per_step > d.nslots)
                 return bfail(nullptr, ISF_ERR_INVALID, who + "emit_per_step must be in 0..nslots");
-            if (d.emit_per_step > 0 && (d.emit_mode < ISF_EMIT_RING || d.emit_mode > ISF_EMIT_CYLINDER))
+            if (d.emit_per_step > 0 && (d.emit_mode < ISF_EMIT_RING || d.emit_mode > ISF_EMIT_RING_PLANE))
                 return bfail(nullptr, ISF_ERR_INVALID, who + "bad emit_mode");
         }
         ClassKey k;

@@ -30,6 +30,8 @@ struct isf_handle {
     cudaEvent_t ev_read[2] = {nullptr, nullptr};  // the advection that read vel_buf[i] is done (side)
     cudaEvent_t ev_side = nullptr;             // the last work queued on side
     bool side_pending = false;                 // side work the main stream has not waited for
+    unsigned* keep_counts = nullptr;           // per-block counts of isf_keep_inside
+    long long keep_cap = 0;
     void* tables = nullptr;  // twiddles, phase factors, Laplacian symbols
     unsigned long long* counters = nullptr;  // [0] clamp events, [1] live particles, [2..] ISF_CHECK record
     unsigned long long launches = 0;         // kernels launched by this handle

@@ -108,6 +108,35 @@ constexpr int kCounterStride = 8;
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel,
                           unsigned long long* counters, cudaStream_t s, int nsim = 1, long long bs_vel = 0);
 
+// the Particles type of MatlabPort.jl: x, y, z vectors and active slot lists (k_particles.cu)
+cudaError_t launch_emit_soa(float* x, float* y, float* z, long long nslots, long long start, long long count,
+                            const EmitArgs& e, cudaStream_t s);
+// counters: [0] clamp events, [1] advected slots, [12] slots outside [0, nslots)
+cudaError_t launch_advect_active(const Grid& g, float* x, float* y, float* z, long long nslots, const long long* active,
+                                 long long n, float dt, const float* vel, unsigned long long* counters, cudaStream_t s);
+cudaError_t launch_sample_velocity(const Grid& g, const float* x, const float* y, const float* z, long long n,
+                                   const float* vel, float* ux, float* uy, float* uz, unsigned long long* counters,
+                                   cudaStream_t s);
+// block count of the keep-inside filter of n items (the size of its counts scratch)
+long long keep_blocks(long long n);
+cudaError_t launch_keep_inside(const Grid& g, const float* x, const float* y, const float* z, long long nslots,
+                               const long long* active, long long n, unsigned* counts, long long* out,
+                               long long* out_n, cudaStream_t s);
+cudaError_t launch_gather3(const float* x, const float* y, const float* z, long long nslots, const long long* ind,
+                           long long n, float* ox, float* oy, float* oz, unsigned long long* counters, cudaStream_t s);
+
+// FP64 structure-of-arrays conversions and the complex gauge (k_soa.cu)
+cudaError_t launch_psi_from_f64(const double* a, const double* b, float* psi, long long n, cudaStream_t s);
+cudaError_t launch_psi_to_f64(const float* psi, double* a, double* b, long long n, cudaStream_t s);
+cudaError_t launch_vel_from_f64(const Grid& g, const double* vx, const double* vy, const double* vz, float* vel,
+                                cudaStream_t s);
+cudaError_t launch_vel_to_f64(const Grid& g, const float* vel, double* vx, double* vy, double* vz, cudaStream_t s);
+cudaError_t launch_real_from_f64(const double* src, long long stride, double scale, float* dst, long long n,
+                                 cudaStream_t s);
+cudaError_t launch_real_to_f64(const float* src, double* dst, long long n, cudaStream_t s);
+cudaError_t launch_complex_to_f64(const float* re, const float* im, double* dst, long long n, cudaStream_t s);
+cudaError_t launch_gauge_complex(float* psi, const float* qre, const float* qim, long long n, cudaStream_t s);
+
 // adjoint kernels (k_adjoint.cu)
 cudaError_t launch_gauge(const Grid& g, const float4* in, const float* q, float4* out, cudaStream_t s);
 cudaError_t launch_normalize_to(const Grid& g, const float4* in, float4* out, cudaStream_t s);

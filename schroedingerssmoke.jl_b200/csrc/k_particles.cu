@@ -34,9 +34,42 @@ __device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0
 // Stream: counter = (j, counter_lo, counter_hi, 0x15F0015F), key = seed.
 // mode 0: the reference ring (0.9 r around (x - 0.1) with +-0.05 jitter,
 //         particles.jl:86-90); 1: uniform in the nozzle disc at x = cen.x;
-//         2: uniform in the nozzle cylinder.
-// A batch launch (emits != null) handles simulation s = blockIdx.y with
-// emits[s] and its own slots parts + s * 3 * nslots.
+//         2: uniform in the nozzle cylinder; 3: the MatlabPort driver's ring
+//         (0.9 r in the plane x = cen.x, no jitter,
+//         examples/matlabport/simple.jl:112-115).
+__device__ __forceinline__ float3 emit_point(long long j, const EmitArgs& e) {
+    U4 c = {{(uint32_t)j, (uint32_t)e.counter, (uint32_t)(e.counter >> 32), 0x15F0015Fu}};
+    const U4 r = philox4x32_10(c, (uint32_t)e.seed, (uint32_t)(e.seed >> 32));
+    const float u0 = u01(r.v[0]), u1 = u01(r.v[1]), u2 = u01(r.v[2]), u3 = u01(r.v[3]);
+    const float pi = 3.14159265358979323846f;
+    float p0, p1, p2;
+    if (e.mode == 0 || e.mode == 3) {
+        const float rt = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
+        const float rr = __fmul_rn(0.9f, e.rad);
+        if (e.mode == 3) {
+            p0 = e.cen[0];
+            p1 = __fadd_rn(e.cen[1], __fmul_rn(rr, cosf(rt)));
+            p2 = __fadd_rn(e.cen[2], __fmul_rn(rr, sinf(rt)));
+        } else {
+            const float o0 = __fsub_rn(__fmul_rn(u1, 0.1f), 0.05f);
+            const float o1 = __fsub_rn(__fmul_rn(u2, 0.1f), 0.05f);
+            const float o2 = __fsub_rn(__fmul_rn(u3, 0.1f), 0.05f);
+            p0 = __fadd_rn(__fsub_rn(e.cen[0], 0.1f), o0);
+            p1 = __fadd_rn(__fadd_rn(e.cen[1], __fmul_rn(rr, cosf(rt))), o1);
+            p2 = __fadd_rn(__fadd_rn(e.cen[2], __fmul_rn(rr, sinf(rt))), o2);
+        }
+    } else {
+        const float th = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
+        const float rho = __fmul_rn(e.rad, sqrtf(u1));
+        p0 = (e.mode == 1) ? e.cen[0] : __fadd_rn(e.cen[0], __fmul_rn(__fsub_rn(u2, 0.5f), e.len));
+        p1 = __fadd_rn(e.cen[1], __fmul_rn(rho, cosf(th)));
+        p2 = __fadd_rn(e.cen[2], __fmul_rn(rho, sinf(th)));
+    }
+    return make_float3(p0, p1, p2);
+}
+
+// Particles of slot array(s) parts; a batch launch (emits != null) handles
+// simulation s = blockIdx.y with emits[s] and its own slots parts + s * 3 * nslots.
 __global__ void k_emit(float* __restrict__ parts, long long nslots, long long start, long long count, EmitArgs e,
                        const EmitState* __restrict__ emits) {
     pdl_enter();
@@ -48,31 +81,24 @@ __global__ void k_emit(float* __restrict__ parts, long long nslots, long long st
         start = st.start;
         parts += blockIdx.y * 3 * nslots;
     }
-    U4 c = {{(uint32_t)j, (uint32_t)e.counter, (uint32_t)(e.counter >> 32), 0x15F0015Fu}};
-    const U4 r = philox4x32_10(c, (uint32_t)e.seed, (uint32_t)(e.seed >> 32));
-    const float u0 = u01(r.v[0]), u1 = u01(r.v[1]), u2 = u01(r.v[2]), u3 = u01(r.v[3]);
-    const float pi = 3.14159265358979323846f;
-    float p0, p1, p2;
-    if (e.mode == 0) {
-        const float rt = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
-        const float o0 = __fsub_rn(__fmul_rn(u1, 0.1f), 0.05f);
-        const float o1 = __fsub_rn(__fmul_rn(u2, 0.1f), 0.05f);
-        const float o2 = __fsub_rn(__fmul_rn(u3, 0.1f), 0.05f);
-        const float rr = __fmul_rn(0.9f, e.rad);
-        p0 = __fadd_rn(__fsub_rn(e.cen[0], 0.1f), o0);
-        p1 = __fadd_rn(__fadd_rn(e.cen[1], __fmul_rn(rr, cosf(rt))), o1);
-        p2 = __fadd_rn(__fadd_rn(e.cen[2], __fmul_rn(rr, sinf(rt))), o2);
-    } else {
-        const float th = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
-        const float rho = __fmul_rn(e.rad, sqrtf(u1));
-        p0 = (e.mode == 1) ? e.cen[0] : __fadd_rn(e.cen[0], __fmul_rn(__fsub_rn(u2, 0.5f), e.len));
-        p1 = __fadd_rn(e.cen[1], __fmul_rn(rho, cosf(th)));
-        p2 = __fadd_rn(e.cen[2], __fmul_rn(rho, sinf(th)));
-    }
+    const float3 p = emit_point(j, e);
     long long s = (start + j) % nslots;
-    parts[3 * s + 0] = p0;
-    parts[3 * s + 1] = p1;
-    parts[3 * s + 2] = p2;
+    parts[3 * s + 0] = p.x;
+    parts[3 * s + 1] = p.y;
+    parts[3 * s + 2] = p.z;
+}
+
+// the same stream into separate x, y, z vectors (the Particles type of MatlabPort.jl:178-196)
+__global__ void k_emit_soa(float* __restrict__ x, float* __restrict__ y, float* __restrict__ z, long long nslots,
+                           long long start, long long count, EmitArgs e) {
+    pdl_enter();
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const float3 p = emit_point(j, e);
+    const long long s = (start + j) % nslots;
+    x[s] = p.x;
+    y[s] = p.y;
+    z[s] = p.z;
 }
 
 #ifdef ISF_CHECK
@@ -203,6 +229,272 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
             if (l) atomicAdd(&counters[1], l);
         }
     }
+}
+
+// ---- the Particles type of MatlabPort.jl (x, y, z vectors and a list of
+// active slots) on the same interpolation
+
+// block-aggregated counter increments: one atomic per CTA
+__device__ __forceinline__ void block_add(unsigned long long* ctr, unsigned v) {
+    __shared__ unsigned red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        if (t) atomicAdd(ctr, t);
+    }
+    __syncthreads();
+}
+
+// StaggeredAdvect (MatlabPort.jl:200-222): RK4 for the slots active[j]
+// (j < n; slot j itself when active is null) with no box test, sample points
+// wrapped by mod inside the interpolation.  Slots outside [0, nslots) are
+// skipped and counted in counters[12]; counters[0] accumulates clamp events,
+// counters[1] advected slots.
+template <bool POW2, bool NORMW>
+__global__ void __launch_bounds__(256) k_advect_active(Grid g, float* __restrict__ x, float* __restrict__ y,
+                                                       float* __restrict__ z, long long nslots,
+                                                       const long long* __restrict__ active, long long n, float dt,
+                                                       const float* __restrict__ vel,
+                                                       unsigned long long* __restrict__ counters) {
+    pdl_enter();
+    const AdvConst kc = adv_const(g, vel);
+    unsigned clamps = 0, moved = 0, bad = 0;
+    unsigned long long* chk = counters + 2;
+    const float s6 = dt / 6.0f;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const long long k = active ? active[j] : j;
+        if (k < 0 || k >= nslots) {
+            ++bad;
+            continue;
+        }
+        ++moved;
+        float3 p = make_float3(x[k], y[k], z[k]);
+        const float3 k1 = stag_vel<POW2, NORMW>(kc, p, clamps, chk);
+        float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
+        const float3 k2 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
+        q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
+        const float3 k3 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
+        q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
+        const float3 k4 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
+        x[k] = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
+        y[k] = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
+        z[k] = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
+    }
+    block_add(&counters[0], clamps);
+    block_add(&counters[1], moved);
+    block_add(&counters[12], bad);
+}
+
+// StaggeredVelocity (MatlabPort.jl:238-273) at n points
+template <bool POW2, bool NORMW>
+__global__ void __launch_bounds__(256) k_sample_vel(Grid g, const float* __restrict__ x, const float* __restrict__ y,
+                                                    const float* __restrict__ z, long long n,
+                                                    const float* __restrict__ vel, float* __restrict__ ux,
+                                                    float* __restrict__ uy, float* __restrict__ uz,
+                                                    unsigned long long* __restrict__ counters) {
+    pdl_enter();
+    const AdvConst kc = adv_const(g, vel);
+    unsigned clamps = 0;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const float3 u = stag_vel<POW2, NORMW>(kc, make_float3(x[j], y[j], z[j]), clamps, counters + 2);
+        ux[j] = u.x;
+        uy[j] = u.y;
+        uz[j] = u.z;
+    }
+    block_add(&counters[0], clamps);
+}
+
+// Order-preserving filter of the active slots whose position is strictly
+// inside the box (removethedead!, examples/matlabport/simple.jl:67-74, with
+// the open-box test of its isinside): per-block counts, one scan, scatter.
+constexpr int KEEP_T = 256, KEEP_V = 4, KEEP_ITEMS = KEEP_T * KEEP_V;
+
+__device__ __forceinline__ bool keep_item(const float* x, const float* y, const float* z, long long nslots,
+                                          const long long* active, long long n, long long j, float L0, float L1,
+                                          float L2, long long* slot) {
+    if (j >= n) return false;
+    const long long k = active ? active[j] : j;
+    *slot = k;
+    if (k < 0 || k >= nslots) return false;
+    const float px = x[k], py = y[k], pz = z[k];
+    return (px > 0.f && px < L0) && (py > 0.f && py < L1) && (pz > 0.f && pz < L2);
+}
+
+__global__ void __launch_bounds__(KEEP_T) k_keep_count(const float* __restrict__ x, const float* __restrict__ y,
+                                                       const float* __restrict__ z, long long nslots,
+                                                       const long long* __restrict__ active, long long n, float L0,
+                                                       float L1, float L2, unsigned* __restrict__ counts) {
+    pdl_enter();
+    const long long base = (long long)blockIdx.x * KEEP_ITEMS + (long long)threadIdx.x * KEEP_V;
+    unsigned c = 0;
+    long long slot;
+#pragma unroll
+    for (int v = 0; v < KEEP_V; ++v) c += keep_item(x, y, z, nslots, active, n, base + v, L0, L1, L2, &slot) ? 1u : 0u;
+    __shared__ unsigned red[KEEP_T / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < KEEP_T / 32; ++w) t += red[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// exclusive scan of nb block counts in place (one CTA of 1024 threads, each
+// summing a contiguous run), the total into *out_n
+__global__ void __launch_bounds__(1024) k_keep_scan(unsigned* __restrict__ counts, long long nb,
+                                                    long long* __restrict__ out_n) {
+    pdl_enter();
+    __shared__ unsigned long long part[1024];
+    const long long per = (nb + 1023) / 1024;
+    const long long b0 = threadIdx.x * per, b1 = min(b0 + per, nb);
+    unsigned long long s = 0;
+    for (long long b = b0; b < b1; ++b) s += counts[b];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {  // Hillis-Steele inclusive scan of the runs
+        const unsigned long long v = threadIdx.x >= o ? part[threadIdx.x - o] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long run = part[threadIdx.x] - s;
+    for (long long b = b0; b < b1; ++b) {
+        const unsigned c = counts[b];
+        counts[b] = (unsigned)run;
+        run += c;
+    }
+    if (threadIdx.x == 1023) *out_n = (long long)part[1023];
+}
+
+__global__ void __launch_bounds__(KEEP_T) k_keep_scatter(const float* __restrict__ x, const float* __restrict__ y,
+                                                         const float* __restrict__ z, long long nslots,
+                                                         const long long* __restrict__ active, long long n, float L0,
+                                                         float L1, float L2, const unsigned* __restrict__ offsets,
+                                                         long long* __restrict__ out) {
+    pdl_enter();
+    const long long base = (long long)blockIdx.x * KEEP_ITEMS + (long long)threadIdx.x * KEEP_V;
+    bool f[KEEP_V];
+    long long slot[KEEP_V];
+    unsigned c = 0;
+#pragma unroll
+    for (int v = 0; v < KEEP_V; ++v) {
+        f[v] = keep_item(x, y, z, nslots, active, n, base + v, L0, L1, L2, &slot[v]);
+        c += f[v] ? 1u : 0u;
+    }
+    // exclusive prefix of c over the block: warp inclusive scan, then warp totals
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    __shared__ unsigned wsum[KEEP_T / 32];
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    unsigned wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += wsum[w];
+    long long pos = (long long)offsets[blockIdx.x] + wbase + inc - c;
+#pragma unroll
+    for (int v = 0; v < KEEP_V; ++v)
+        if (f[v]) out[pos++] = slot[v];
+}
+
+// Keep(particle, ind) (MatlabPort.jl:228-233): o[i] = p[ind[i]]; an index
+// outside [0, nslots) gives (-1, -1, -1) and is counted in counters[12]
+__global__ void __launch_bounds__(256) k_gather3(const float* __restrict__ x, const float* __restrict__ y,
+                                                 const float* __restrict__ z, long long nslots,
+                                                 const long long* __restrict__ ind, long long n,
+                                                 float* __restrict__ ox, float* __restrict__ oy,
+                                                 float* __restrict__ oz, unsigned long long* __restrict__ counters) {
+    pdl_enter();
+    unsigned bad = 0;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const long long k = ind[j];
+        const bool ok = k >= 0 && k < nslots;
+        bad += ok ? 0u : 1u;
+        ox[j] = ok ? x[k] : -1.f;
+        oy[j] = ok ? y[k] : -1.f;
+        oz[j] = ok ? z[k] : -1.f;
+    }
+    block_add(&counters[12], bad);
+}
+
+namespace {
+unsigned grid_for(long long n, int blk) {
+    long long b = (n + blk - 1) / blk;
+    if (b > 148LL * 64) b = 148LL * 64;
+    return (unsigned)(b > 0 ? b : 1);
+}
+}  // namespace
+
+cudaError_t launch_emit_soa(float* x, float* y, float* z, long long nslots, long long start, long long count,
+                            const EmitArgs& e, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    const int blk = 256;
+    return launch_pdl(k_emit_soa, dim3((unsigned)((count + blk - 1) / blk)), dim3(blk), 0, s, x, y, z, nslots, start,
+                      count, e);
+}
+
+cudaError_t launch_advect_active(const Grid& g, float* x, float* y, float* z, long long nslots, const long long* active,
+                                 long long n, float dt, const float* vel, unsigned long long* counters, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const dim3 grid(grid_for(n, 256));
+    const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
+    if (g.norm_w)
+        return pow2 ? launch_pdl(k_advect_active<true, true>, grid, dim3(256), 0, s, g, x, y, z, nslots, active, n, dt,
+                                 vel, counters)
+                    : launch_pdl(k_advect_active<false, true>, grid, dim3(256), 0, s, g, x, y, z, nslots, active, n, dt,
+                                 vel, counters);
+    return pow2 ? launch_pdl(k_advect_active<true, false>, grid, dim3(256), 0, s, g, x, y, z, nslots, active, n, dt,
+                             vel, counters)
+                : launch_pdl(k_advect_active<false, false>, grid, dim3(256), 0, s, g, x, y, z, nslots, active, n, dt,
+                             vel, counters);
+}
+
+cudaError_t launch_sample_velocity(const Grid& g, const float* x, const float* y, const float* z, long long n,
+                                   const float* vel, float* ux, float* uy, float* uz, unsigned long long* counters,
+                                   cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const dim3 grid(grid_for(n, 256));
+    const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
+    if (g.norm_w)
+        return pow2 ? launch_pdl(k_sample_vel<true, true>, grid, dim3(256), 0, s, g, x, y, z, n, vel, ux, uy, uz, counters)
+                    : launch_pdl(k_sample_vel<false, true>, grid, dim3(256), 0, s, g, x, y, z, n, vel, ux, uy, uz,
+                                 counters);
+    return pow2 ? launch_pdl(k_sample_vel<true, false>, grid, dim3(256), 0, s, g, x, y, z, n, vel, ux, uy, uz, counters)
+                : launch_pdl(k_sample_vel<false, false>, grid, dim3(256), 0, s, g, x, y, z, n, vel, ux, uy, uz, counters);
+}
+
+long long keep_blocks(long long n) { return (n + KEEP_ITEMS - 1) / KEEP_ITEMS; }
+
+cudaError_t launch_keep_inside(const Grid& g, const float* x, const float* y, const float* z, long long nslots,
+                               const long long* active, long long n, unsigned* counts, long long* out,
+                               long long* out_n, cudaStream_t s) {
+    const long long nb = keep_blocks(n);
+    if (nb == 0) return cudaMemsetAsync(out_n, 0, sizeof(long long), s);
+    const float L0 = g.L[0], L1 = g.L[1], L2 = g.L[2];
+    cudaError_t e = launch_pdl(k_keep_count, dim3((unsigned)nb), dim3(KEEP_T), 0, s, x, y, z, nslots, active, n, L0, L1,
+                               L2, counts);
+    if (e == cudaSuccess) e = launch_pdl(k_keep_scan, dim3(1), dim3(1024), 0, s, counts, nb, out_n);
+    if (e == cudaSuccess)
+        e = launch_pdl(k_keep_scatter, dim3((unsigned)nb), dim3(KEEP_T), 0, s, x, y, z, nslots, active, n, L0, L1, L2,
+                       (const unsigned*)counts, out);
+    return e;
+}
+
+cudaError_t launch_gather3(const float* x, const float* y, const float* z, long long nslots, const long long* ind,
+                           long long n, float* ox, float* oy, float* oz, unsigned long long* counters, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    return launch_pdl(k_gather3, dim3(grid_for(n, 256)), dim3(256), 0, s, x, y, z, nslots, ind, n, ox, oy, oz,
+                      counters);
 }
 
 cudaError_t launch_emit(float* parts, long long nslots, long long start, long long count, const EmitArgs& e,

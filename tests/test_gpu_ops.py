@@ -168,7 +168,7 @@ def test_restrict_velocity(isfpkg, oracle_mod, cfgs, phase_mode, use_mask):
     assert rel(host(psi), psi64) < 2e-6
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
 def test_add_particles(isfpkg, oracle_mod, cfgs, mode):
     L, dims = (4, 2, 2), (64, 32, 32)
     isf = isfpkg.ISF(L, dims, HBAR, DT)

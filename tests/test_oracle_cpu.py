@@ -231,7 +231,7 @@ def test_emission_modes_geometry(oracle_mod):
     L, dims = (4, 2, 2), (32, 16, 16)
     o = oracle_mod.Oracle(L, dims, HBAR, DT)
     cen = (0.3, 0.966, 1.066)
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3):
         p = np.full((2000, 3), -1.0)
         o.add_particles(p, 0, 2000, cen, 0.5, seed=1, counter=0, mode=mode, length=0.5)
         r = np.hypot(p[:, 1] - cen[1], p[:, 2] - cen[2])
@@ -240,5 +240,25 @@ def test_emission_modes_geometry(oracle_mod):
             assert (np.abs(r - 0.45) <= 0.05 * np.sqrt(2) + 1e-9).all()
         elif mode == 1:
             assert (p[:, 0] == np.float64(np.float32(cen[0]))).all() and (r <= 0.5 + 1e-9).all()
+        elif mode == 3:   # MatlabPort driver ring: 0.9 r in the plane x = cen.x (simple.jl:112-115)
+            assert (p[:, 0] == np.float64(np.float32(cen[0]))).all() and np.abs(r - 0.45).max() < 1e-6
         else:
             assert (np.abs(p[:, 0] - cen[0]) <= 0.25 + 1e-6).all() and (r <= 0.5 + 1e-9).all()
+
+
+def test_matlabport_driver_step_particle_semantics():
+    """oracle.matlabport.driver_step: psi as jet_step; births appended and
+    active; slots outside the box leave the active list and are not moved;
+    the others move by StaggeredAdvect."""
+    L, dims = (4, 2, 2), (32, 16, 16)
+    oo = mp.MatlabISF(L, dims, HBAR, DT)
+    isjet = mp.is_jet(oo, (0.3, 0.966, 1.066), 0.5, 0.5)
+    p1, p2 = mp.from_aos(smooth_psi(dims, seed=2))
+    x, y, z = (np.full(100, 1.0, np.float32) for _ in range(3))
+    x[1] = -0.5                                     # outside: dropped from the list, kept as is
+    births = (np.float32([0.3, 0.3]), np.float32([0.9, 1.0]), np.float32([1.0, 1.1]))
+    a1, a2, n, act = mp.driver_step(oo, p1, p2, isjet, (10, 0, 0), 0.1, x, y, z, 3, np.arange(3), births)
+    b1, b2, _ = mp.jet_step(oo, p1, p2, isjet, (10, 0, 0), 0.1)
+    assert rel(a1, b1) == 0 and rel(a2, b2) == 0
+    assert n == 5 and list(act) == [0, 2, 3, 4]
+    assert x[1] == -0.5 and (x[[0, 2]] != 1.0).all()
