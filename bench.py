@@ -534,6 +534,9 @@ def main():
     isf.profile_start()
     for _ in range(args.steps):
         pkg.step(isf, psi, parts, None)
+        # each launch timed alone: the advection on the particle stream is
+        # joined before the next step's passes are queued
+        isf.join()
     sites = isf.profile_stop()
     total_site_ms = sum(v[0] for v in sites.values())
     dom = max(sites, key=lambda k: sites[k][0])
