@@ -181,10 +181,12 @@ __device__ __forceinline__ bool restrict_cell(const Grid& g, const JetArgs& j, i
     return true;
 }
 
-// normalize_psi (parallel.jl:162-165)
+// normalize_psi (parallel.jl:162-165): psi * (1 / |psi|) with the
+// reciprocal square root rounded once, then four products (within 1.5 ulp of
+// the four quotients psi / |psi|, at a quarter of their instructions)
 __device__ __forceinline__ float4 normalize4(float4 v) {
-    const float nrm = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
-    return make_float4(__fdiv_rn(v.x, nrm), __fdiv_rn(v.y, nrm), __fdiv_rn(v.z, nrm), __fdiv_rn(v.w, nrm));
+    const float r = __frsqrt_rn(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
+    return make_float4(v.x * r, v.y * r, v.z * r, v.w * r);
 }
 
 // gauge_transform (parallel.jl:125-129) with real q: psi * exp(-i q)
