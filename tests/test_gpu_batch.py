@@ -109,6 +109,7 @@ def test_batch_step_counter_and_restart(isfpkg, cfgs):
     b.sync()
     for i in range(len(sims)):
         assert torch.equal(a.psi(i), b.psi(i)), i
+        assert torch.equal(a.particles(i), b.particles(i)), i
     # restart from step 3's state with the counter at 3
     c = batch_run(isfpkg, sims, psi0, parts0, 2, 3, tune=False)
     psi3 = [c.psi(i) for i in range(len(sims))]
