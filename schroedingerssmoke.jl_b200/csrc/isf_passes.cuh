@@ -281,27 +281,11 @@ __global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs 
     float2* tile = plane + N * N + grp * (N * C);
     const int kx = blockIdx.x;
     float2* __restrict__ Fp = a.F + blockIdx.y * a.bs_F + (long long)kx * N * N;
-    constexpr int NV = N * N / 2, VIT = (NV + Sh::BLK - 1) / Sh::BLK;  // float4 per plane, per thread
-    {
-        // all of a thread's loads in flight at once
-        const float4* __restrict__ s4 = reinterpret_cast<const float4*>(Fp);
-        float4* p4 = reinterpret_cast<float4*>(plane);
-        float4 v[VIT];
-#pragma unroll
-        for (int it = 0; it < VIT; ++it) {
-            const int i = it * Sh::BLK + threadIdx.x;
-            if (i < NV) v[it] = s4[i];
-        }
-#pragma unroll
-        for (int it = 0; it < VIT; ++it) {
-            const int i = it * Sh::BLK + threadIdx.x;
-            if (i < NV) p4[i] = v[it];
-        }
-    }
-    __syncthreads();
     float2 x[Plan<N>::EMAX];
     const float2 zero = make_float2(0.f, 0.f);
-    // y transforms: pencil = row z of the plane, lanes along y
+    // y transforms: pencil = row z of the plane, lanes along y.  The forward
+    // one reads its rows straight from HBM into registers and leaves them in
+    // shared memory; the inverse one reads shared memory and writes HBM.
     auto ysweep = [&](auto sign) {
         constexpr int S = decltype(sign)::value;
         const int t = lt % NT, q = lt / NT;
@@ -309,9 +293,16 @@ __global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs 
         for (int round = 0; round < Sh::ROUNDS; ++round) {
             const int z = (round * Sh::GROUPS + grp) * C + q;
             const bool on = z < N;
-            auto src = [&](int j) -> float2 { return on ? plane[z * N + j] : zero; };
+            auto src = [&](int j) -> float2 {
+                if (S < 0) return on ? Fp[z * N + j] : zero;
+                return on ? plane[z * N + j] : zero;
+            };
             auto dst = [&](int j, const float2& v) {
-                if (on) plane[z * N + j] = v;
+                if (!on) return;
+                if (S < 0)
+                    plane[z * N + j] = v;
+                else
+                    Fp[z * N + j] = v;
             };
             Plan<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst);
             __syncthreads();
@@ -346,15 +337,6 @@ __global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs 
         }
     }
     ysweep(std::integral_constant<int, +1>());
-    {
-        float4* __restrict__ d4 = reinterpret_cast<float4*>(Fp);
-        const float4* p4 = reinterpret_cast<const float4*>(plane);
-#pragma unroll
-        for (int it = 0; it < VIT; ++it) {
-            const int i = it * Sh::BLK + threadIdx.x;
-            if (i < NV) d4[i] = p4[i];
-        }
-    }
 }
 
 // -------------------------------------------------------------- y / z pass
