@@ -13,7 +13,7 @@ lines): Schroedinger flow, normalize, pressure projection, velocity one-form
 Printed JSON (rank 0): value = steps/s of the whole job (N independent
 replicas for N > 1, "scaling": "weak"), timed with CUDA events on the
 library's stream over exactly K steps after W warm-up steps, max over ranks.
-The working set (psi 64 MiB, velocity 49 MiB, particles 48 MiB, divergence
+The working set (psi 64 MiB, velocity 65 MiB, particles 48 MiB, divergence
 16 MiB, half spectrum 18 MiB) is larger than the 126 MB L2, so no flush is
 needed between steps.
 
@@ -615,7 +615,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": list(c["dims"]), "torus": list(c["L"]), "hbar": c["hbar"],
                    "dt": c["dt"], "particles": P, "jet": False,
-                   "l2": "inputs larger than L2: psi 64 MiB + velocity 49 MiB + particles 48 MiB + f 16 MiB + half spectrum 18 MiB",
+                   "l2": "inputs larger than L2: psi 64 MiB + velocity 65 MiB + particles 48 MiB + f 16 MiB + half spectrum 18 MiB",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

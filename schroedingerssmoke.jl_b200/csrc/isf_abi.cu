@@ -10,7 +10,7 @@
 #include "../../include/isf.h"
 #include "isf_handle.h"
 
-// row pitch (floats) of the padded velocity planes is a multiple of this
+// row pitch (cells) of the padded velocity grid is a multiple of this
 #ifndef ISF_VEL_ROW_ALIGN
 #define ISF_VEL_ROW_ALIGN 1
 #endif
@@ -255,7 +255,7 @@ StencilArgs stargs(isf_handle* h, const float* psi, float* out) {
 }
 
 // velocity_one_form!(isf, psi, hbar) [+ staggered sharp] into the handle's
-// velocity: the plane set no in-flight advection reads, which becomes current
+// velocity: the grid no in-flight advection reads, which becomes current
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site) {
     const int nb = h->vcur ^ 1;
     if (h->side) ISF_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_read[nb], 0), "velocity buffer reuse");
@@ -374,8 +374,8 @@ int isf_create(const isf_params* p, isf_handle** out) {
         if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: particle stream: ") + cudaGetErrorString(e));
     }
     if (cudaMalloc(&h->F, sizeof(float2) * g.N) != cudaSuccess || cudaMalloc(&h->f, sizeof(float) * g.N) != cudaSuccess ||
-        cudaMalloc(&h->vel_buf[0], sizeof(float) * 3 * g.NP) != cudaSuccess ||
-        cudaMalloc(&h->vel_buf[1], sizeof(float) * 3 * g.NP) != cudaSuccess ||
+        cudaMalloc(&h->vel_buf[0], sizeof(float) * kVelComp * g.NP) != cudaSuccess ||
+        cudaMalloc(&h->vel_buf[1], sizeof(float) * kVelComp * g.NP) != cudaSuccess ||
         cudaMalloc(&h->tables, total) != cudaSuccess ||
         cudaMalloc(&h->counters, 16 * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
@@ -383,7 +383,7 @@ int isf_create(const isf_params* p, isf_handle** out) {
     }
     e = cudaMemcpy(h->tables, host.data(), total, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 16 * sizeof(unsigned long long));
-    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemset(h->vel_buf[i], 0, sizeof(float) * 3 * g.NP);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemset(h->vel_buf[i], 0, sizeof(float) * kVelComp * g.NP);
     h->vel = h->vel_buf[0];
     if (e == cudaSuccess) e = cudaMemset(h->F, 0, sizeof(float2) * g.N);
     if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: upload: ") + cudaGetErrorString(e));
@@ -601,7 +601,7 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     // add_particles! (before the projections in the reference; the particles
     // are independent of psi) and staggered_advect!.  With a particle stream
     // they run there, after this step's velocity, while the caller queues the
-    // next step's psi passes; the velocity plane set they read is not written
+    // next step's psi passes; the velocity grid they read is not written
     // again until they are done (run_one_form alternates between two).
     cudaStream_t ps = h->side ? h->side : h->stream;
     const bool emit = a->jet && a->emit_count > 0;

@@ -375,7 +375,7 @@ int isf_adj_get_velocity_bar(isf_handle* h, float* aos) {
     if (!aos) return fail(h, ISF_ERR_INVALID, "isf_adj_get_velocity_bar: null output");
     if (int rc = adj_ensure(h)) return rc;
     ISF_LAUNCH(h, launch_adj_fold(h->g, h->adj->ubar, h->stream), "adj fold");
-    ISF_LAUNCH(h, launch_vel_to_aos(h->g, h->adj->ubar, aos, h->stream), "adj velocity cotangent to aos");
+    ISF_LAUNCH(h, launch_adj_to_aos(h->g, h->adj->ubar, aos, h->stream), "adj velocity cotangent to aos");
     return ISF_OK;
 }
 

@@ -81,7 +81,7 @@ struct BatchClass {
     float4* psi = nullptr;         // nsim x N
     float2* F = nullptr;           // nsim x wp*ny*nz
     float* f = nullptr;            // nsim x N
-    float* vel = nullptr;          // nsim x 3 NP
+    float* vel = nullptr;          // nsim x kVelComp NP
     float* parts = nullptr;        // nsim x 3 nslots
     char* tables = nullptr;
     cudaStream_t stream = nullptr;
@@ -244,13 +244,13 @@ cudaError_t class_step(const isf_batch* b, const BatchClass& c, cudaStream_t s) 
                 return e;
         if ((e = class_projection(c, b->jets + c.first, s)) != cudaSuccess) return e;
     }
-    StencilArgs va = bst(c, c.vel, 3 * c.g.NP);
+    StencilArgs va = bst(c, c.vel, kVelComp * c.g.NP);
     va.hbar = c.g.hbar;
     va.sharp = 1;
     if ((e = launch_stencil(ST_VEL, va, s)) != cudaSuccess) return e;
     if (c.key.nslots > 0)
         if ((e = launch_advect(c.g, c.parts, c.key.nslots, c.vel, b->counters + (size_t)c.first * kCounterStride, s,
-                               c.nsim, 3 * c.g.NP)) != cudaSuccess)
+                               c.nsim, kVelComp * c.g.NP)) != cudaSuccess)
             return e;
     return cudaSuccess;
 }
@@ -489,7 +489,7 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
         if (cudaMalloc(&c.psi, sizeof(float4) * c.g.N * ns) != cudaSuccess ||
             cudaMalloc(&c.F, sizeof(float2) * c.bs_F() * ns) != cudaSuccess ||
             cudaMalloc(&c.f, sizeof(float) * c.g.N * ns) != cudaSuccess ||
-            cudaMalloc(&c.vel, sizeof(float) * 3 * c.g.NP * ns) != cudaSuccess ||
+            cudaMalloc(&c.vel, sizeof(float) * kVelComp * c.g.NP * ns) != cudaSuccess ||
             (c.key.nslots > 0 && cudaMalloc(&c.parts, sizeof(float) * 3 * c.key.nslots * ns) != cudaSuccess) ||
             cudaMalloc(&c.tables, host.size()) != cudaSuccess) {
             cudaGetLastError();
@@ -539,7 +539,7 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
         cudaError_t r = cudaMemsetAsync(c.psi, 0, sizeof(float4) * c.g.N * ns, b->stream);
         if (r == cudaSuccess) r = cudaMemsetAsync(c.F, 0, sizeof(float2) * c.bs_F() * ns, b->stream);
         if (r == cudaSuccess) r = cudaMemsetAsync(c.f, 0, sizeof(float) * c.g.N * ns, b->stream);
-        if (r == cudaSuccess) r = cudaMemsetAsync(c.vel, 0, sizeof(float) * 3 * c.g.NP * ns, b->stream);
+        if (r == cudaSuccess) r = cudaMemsetAsync(c.vel, 0, sizeof(float) * kVelComp * c.g.NP * ns, b->stream);
         if (r == cudaSuccess && c.parts) {
             const long long n = 3 * c.key.nslots * (long long)ns;
             k_fill<<<(unsigned)std::min<long long>((n + 255) / 256, 148LL * 16), 256, 0, b->stream>>>(c.parts, n, -1.f);

@@ -4,11 +4,12 @@
 //   cell index  c = x + nx*(y + ny*z)  (column-major, x fastest)
 //   psi         float4 per cell = (re psi1, im psi1, re psi2, im psi2)
 //               == NTuple{2,ComplexF32} of src/parallel.jl
-//   velocity    three planes vx | vy | vz (internal to the handle), each
-//               (nx+1) x (ny+1) x (nz+1) cells with
+//   velocity    one float4 (vx, vy, vz, 0) per cell of a padded
+//               (nx+1) x (ny+1) x (nz+1) grid (internal to the handle), with
 //               a periodic copy of the x = 0, y = 0 and z = 0 faces at x = nx,
 //               y = ny, z = nz, so the +1 neighbour of any cell is a fixed
-//               offset (+1, +pnx, +pnxy)
+//               offset (+1, +pnx, +pnxy) and one 16-byte load gives all three
+//               components of a cell
 //   F           float2 per cell: the Poisson spectrum work array
 //   particles   float3 per slot (AoS), dead slot = (-1,-1,-1)
 #pragma once
@@ -31,37 +32,41 @@ struct Grid {
     const double2* mtab[3]; // per-axis Schroedinger phase factors exp(i th_a(k))
     const double* s2[3];    // (sin(pi k / n_a) / d_a)^2 in double
     double invN;            // 1 / N
-    int pnx, pnxy;          // strides of the padded velocity planes: nx+1 (rounded up to the row alignment), pnx (ny+1)
-    long long NP;           // cells of one padded velocity plane
+    int pnx, pnxy;          // strides of the padded velocity grid: nx+1 (rounded up to the row alignment), pnx (ny+1)
+    long long NP;           // cells of the padded velocity grid (float4 each)
     int norm_w;             // staggered interpolation weights divided by d (ISF_FLAG_NORMALIZED_WEIGHTS)
 };
 
-// index of cell (x, y, z), 0 <= x <= nx etc., in a padded velocity plane
+// floats per padded velocity cell: vx, vy, vz and one unused
+constexpr int kVelComp = 4;
+
+// index of cell (x, y, z), 0 <= x <= nx etc., in the padded velocity grid
 __host__ __device__ __forceinline__ int pcell(const Grid& g, int x, int y, int z) {
     return x + g.pnx * y + g.pnxy * z;
 }
 
-// the periodic copies on the +faces of a padded velocity plane of the value
+// the periodic copies on the +faces of the padded velocity grid of the value
 // at cell index pc (x == 0: cx, ...): seven predicated stores at the fixed
 // offsets ox = nx, oy = ny pnx, oz = nz pnxy
-__device__ __forceinline__ void pcopies(float* __restrict__ plane, int pc, bool cx, bool cy, bool cz, int ox, int oy,
-                                        int oz, float v) {
-    if (cx) plane[pc + ox] = v;
-    if (cy) plane[pc + oy] = v;
-    if (cz) plane[pc + oz] = v;
-    if (cx & cy) plane[pc + ox + oy] = v;
-    if (cx & cz) plane[pc + ox + oz] = v;
-    if (cy & cz) plane[pc + oy + oz] = v;
-    if (cx & cy & cz) plane[pc + ox + oy + oz] = v;
+__device__ __forceinline__ void pcopies(float4* __restrict__ vel, int pc, bool cx, bool cy, bool cz, int ox, int oy,
+                                        int oz, float4 v) {
+    if (cx) vel[pc + ox] = v;
+    if (cy) vel[pc + oy] = v;
+    if (cz) vel[pc + oz] = v;
+    if (cx & cy) vel[pc + ox + oy] = v;
+    if (cx & cz) vel[pc + ox + oz] = v;
+    if (cy & cz) vel[pc + oy + oz] = v;
+    if (cx & cy & cz) vel[pc + ox + oy + oz] = v;
 }
 
-// store v at cell (x, y, z) of a padded velocity plane and at its periodic
-// copies on the +faces (only cells on a low face have copies)
-__device__ __forceinline__ void pstore(const Grid& g, float* __restrict__ plane, int x, int y, int z, float v) {
+// store the velocity v of cell (x, y, z) and its periodic copies on the
+// +faces (only cells on a low face have copies)
+__device__ __forceinline__ void pstore(const Grid& g, float4* __restrict__ vel, int x, int y, int z, float3 v) {
     const int pc = pcell(g, x, y, z);
-    plane[pc] = v;
+    const float4 w = make_float4(v.x, v.y, v.z, 0.f);
+    vel[pc] = w;
     const bool cx = x == 0, cy = y == 0, cz = z == 0;
-    if (cx | cy | cz) pcopies(plane, pc, cx, cy, cz, g.n[0], g.n[1] * g.pnx, g.n[2] * g.pnxy, v);
+    if (cx | cy | cz) pcopies(vel, pc, cx, cy, cz, g.n[0], g.n[1] * g.pnx, g.n[2] * g.pnxy, w);
 }
 
 // Programmatic dependent launch: a kernel launched with programmatic stream

@@ -20,8 +20,8 @@ struct isf_handle {
     int flags = 0;           // ISF_FLAG_* of isf_create
     int kmajor = 0;          // the half spectrum is k-major and solved plane by plane (plane_supported)
     float* f = nullptr;      // divergence of the one-form (isf.f, parallel.jl:29), N
-    float* vel = nullptr;    // the current padded velocity planes vx | vy | vz (3 NP): vel_buf[vcur]
-    float* vel_buf[2] = {nullptr, nullptr};  // two plane sets: a step writes one while the
+    float* vel = nullptr;    // the current padded velocity grid, float4 per cell (kVelComp NP floats): vel_buf[vcur]
+    float* vel_buf[2] = {nullptr, nullptr};  // two velocity grids: a step writes one while the
     int vcur = 0;                            // previous step's advection may still read the other
     // isf_step runs its particle work (emission, advection) on `side`, so the
     // next step's psi passes overlap it; only for handles that own their stream

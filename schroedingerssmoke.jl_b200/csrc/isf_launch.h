@@ -59,7 +59,7 @@ enum StOp { ST_DIV = 0, ST_VEL = 1 };
 struct StencilArgs {
     Grid g;
     const float4* psi;
-    float* out;  // ST_DIV: f[N]; ST_VEL: padded vx | vy | vz planes (3 NP)
+    float* out;  // ST_DIV: f[N]; ST_VEL: padded velocity grid, float4 (vx, vy, vz, 0) per cell (kVelComp NP floats)
     JetArgs jet;
     int use_jet;
     float hbar;
@@ -150,6 +150,7 @@ cudaError_t launch_adj_oneform_vel(const Grid& g, const float4* psi, float4* bar
                                    cudaStream_t s);
 cudaError_t launch_adj_fold(const Grid& g, float* ubar, cudaStream_t s);
 cudaError_t launch_adj_from_aos(const Grid& g, const float* aos, float* ubar, cudaStream_t s);
+cudaError_t launch_adj_to_aos(const Grid& g, const float* ubar, float* aos, cudaStream_t s);
 // acc[0..2] += cotangent of kvec, acc[3] += cotangent of omega t times wscale
 cudaError_t launch_adj_restrict(const Grid& g, const float4* psi_in, float4* bar, const JetArgs& j, double* acc,
                                 float wscale, cudaStream_t s);

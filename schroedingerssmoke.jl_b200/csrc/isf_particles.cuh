@@ -40,9 +40,7 @@ struct AdvConst {
     float L[3], d[3], dinv[3], feps[3];
     int nm[3];  // n - 1
     int pnx, pnxy;
-    const float* __restrict__ vx;
-    const float* __restrict__ vy;
-    const float* __restrict__ vz;
+    const float4* __restrict__ v;  // (vx, vy, vz, 0) per padded cell
     long long NP;
 };
 
@@ -58,9 +56,7 @@ __device__ __forceinline__ AdvConst adv_const(const Grid& g, const float* vel) {
     }
     c.pnx = g.pnx;
     c.pnxy = g.pnxy;
-    c.vx = vel;
-    c.vy = vel + g.NP;
-    c.vz = vel + 2 * g.NP;
+    c.v = reinterpret_cast<const float4*>(vel);
     c.NP = g.NP;
     return c;
 }

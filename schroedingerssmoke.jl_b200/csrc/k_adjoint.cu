@@ -300,18 +300,21 @@ __device__ __forceinline__ void stag_sample(const AdvConst& k, float3 pt, Sample
     const int c000 = i[0] + sy * i[1] + sz * i[2];
     S.c000 = c000;
     const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
-    S.v[0] = __ldg(k.vx + c000);
-    S.v[1] = __ldg(k.vx + c010);
-    S.v[2] = __ldg(k.vx + c001);
-    S.v[3] = __ldg(k.vx + c010 + sz);
-    S.v[4] = __ldg(k.vy + c000);
-    S.v[5] = __ldg(k.vy + c100);
-    S.v[6] = __ldg(k.vy + c001);
-    S.v[7] = __ldg(k.vy + c100 + sz);
-    S.v[8] = __ldg(k.vz + c000);
-    S.v[9] = __ldg(k.vz + c100);
-    S.v[10] = __ldg(k.vz + c010);
-    S.v[11] = __ldg(k.vz + c100 + sy);
+    const float4 a000 = __ldg(k.v + c000), a100 = __ldg(k.v + c100), a010 = __ldg(k.v + c010);
+    const float4 a001 = __ldg(k.v + c001), a011 = __ldg(k.v + c010 + sz), a101 = __ldg(k.v + c100 + sz);
+    const float4 a110 = __ldg(k.v + c100 + sy);
+    S.v[0] = a000.x;
+    S.v[1] = a010.x;
+    S.v[2] = a001.x;
+    S.v[3] = a011.x;
+    S.v[4] = a000.y;
+    S.v[5] = a100.y;
+    S.v[6] = a001.y;
+    S.v[7] = a101.y;
+    S.v[8] = a000.z;
+    S.v[9] = a100.z;
+    S.v[10] = a010.z;
+    S.v[11] = a110.z;
     const float wx = S.w[0], wy = S.w[1], wz = S.w[2];
     S.u.x = (1.f - wz) * ((1.f - wy) * S.v[0] + wy * S.v[1]) + wz * ((1.f - wy) * S.v[2] + wy * S.v[3]);
     S.u.y = (1.f - wz) * ((1.f - wx) * S.v[4] + wx * S.v[5]) + wz * ((1.f - wx) * S.v[6] + wx * S.v[7]);
@@ -319,7 +322,7 @@ __device__ __forceinline__ void stag_sample(const AdvConst& k, float3 pt, Sample
 }
 
 // adjoint of one sample: ub = cotangent of u; returns the cotangent of the
-// sample point and scatters ub times the weights into the velocity planes
+// sample point and scatters ub times the weights into the velocity cotangent planes
 template <bool NORMW>
 __device__ __forceinline__ float3 stag_sample_adj(const AdvConst& k, const Sample& S, float3 ub, float* ubx, float* uby,
                                                   float* ubz) {
@@ -453,6 +456,18 @@ __global__ void k_adj_from_aos(Grid g, const float* __restrict__ aos, float* __r
     }
 }
 
+// the velocity cotangent (three padded planes, folded) as AoS float3 per cell
+__global__ void k_adj_to_aos(Grid g, const float* __restrict__ ubar, float* __restrict__ aos) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
+        int x, y, z;
+        decode_cell(g, c, x, y, z);
+        const int pc = pcell(g, x, y, z);
+        aos[3 * c] = ubar[pc];
+        aos[3 * c + 1] = ubar[g.NP + pc];
+        aos[3 * c + 2] = ubar[2 * g.NP + pc];
+    }
+}
+
 // cotangent 0 for the ring slots an emission overwrote
 __global__ void k_zero_slots(float* __restrict__ lam, long long nslots, long long start, long long count) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -543,6 +558,10 @@ cudaError_t launch_loss(const float* x, const float* y, float* lam, long long np
 }
 cudaError_t launch_adj_from_aos(const Grid& g, const float* aos, float* ubar, cudaStream_t s) {
     k_adj_from_aos<<<grid_n(g.N, 256), 256, 0, s>>>(g, aos, ubar);
+    return cudaGetLastError();
+}
+cudaError_t launch_adj_to_aos(const Grid& g, const float* ubar, float* aos, cudaStream_t s) {
+    k_adj_to_aos<<<grid_n(g.N, 256), 256, 0, s>>>(g, ubar, aos);
     return cudaGetLastError();
 }
 cudaError_t launch_zero_slots(float* lam, long long nslots, long long start, long long count, cudaStream_t s) {

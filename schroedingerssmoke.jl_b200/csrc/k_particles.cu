@@ -119,7 +119,8 @@ __device__ __forceinline__ int checked(const AdvConst& k, int c, unsigned long l
 #endif
 
 // staggered_velocity (parallel.jl:219-246) on the handle's padded velocity
-// planes.  Interpolation weights are the reference's unnormalised
+// grid: seven 16-byte gathers (the cells whose components the reference's
+// twelve samples need).  Interpolation weights are the reference's unnormalised
 // w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
 // clamped to the last cell and counted.
 template <bool POW2, bool NORMW>
@@ -148,13 +149,14 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
     const int sy = k.pnx, sz = k.pnxy;
     const int c000 = i[0] + sy * i[1] + sz * i[2];
     const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
-    // 12 scalar gathers (parallel.jl:224-234)
-    const float x00 = __ldg(k.vx + ISF_IDX(c000)), x10 = __ldg(k.vx + ISF_IDX(c010));
-    const float x01 = __ldg(k.vx + ISF_IDX(c001)), x11 = __ldg(k.vx + ISF_IDX(c010 + sz));
-    const float y00 = __ldg(k.vy + ISF_IDX(c000)), y10 = __ldg(k.vy + ISF_IDX(c100));
-    const float y01 = __ldg(k.vy + ISF_IDX(c001)), y11 = __ldg(k.vy + ISF_IDX(c100 + sz));
-    const float z00 = __ldg(k.vz + ISF_IDX(c000)), z10 = __ldg(k.vz + ISF_IDX(c100));
-    const float z01 = __ldg(k.vz + ISF_IDX(c010)), z11 = __ldg(k.vz + ISF_IDX(c100 + sy));
+    // the reference's 12 samples (parallel.jl:224-234) from 7 cells
+    const float4 a000 = __ldg(k.v + ISF_IDX(c000)), a100 = __ldg(k.v + ISF_IDX(c100));
+    const float4 a010 = __ldg(k.v + ISF_IDX(c010)), a001 = __ldg(k.v + ISF_IDX(c001));
+    const float4 a011 = __ldg(k.v + ISF_IDX(c010 + sz)), a101 = __ldg(k.v + ISF_IDX(c100 + sz));
+    const float4 a110 = __ldg(k.v + ISF_IDX(c100 + sy));
+    const float x00 = a000.x, x10 = a010.x, x01 = a001.x, x11 = a011.x;
+    const float y00 = a000.y, y10 = a100.y, y01 = a001.y, y11 = a101.y;
+    const float z00 = a000.z, z10 = a100.z, z01 = a010.z, z11 = a110.z;
     const float wx = w[0], wy = w[1], wz = w[2];
     float3 u;
     // u_x bilinear in (y, z), u_y in (x, z), u_z in (x, y) (parallel.jl:230-245)

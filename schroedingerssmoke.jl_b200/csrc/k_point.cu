@@ -1,7 +1,7 @@
 // Pointwise and nearest-neighbour kernels of the ISF API that are not fused
 // into an FFT pass or a stencil: the standalone forms of normalize_psi,
 // restrict_velocity!, isjet, the staggered sharp and div! (from the velocity
-// planes), and layout conversions of the handle's velocity planes.
+// grid), and layout conversions of the handle's padded velocity grid.
 #include "isf_launch.h"
 
 namespace isf {
@@ -42,11 +42,15 @@ __global__ void k_isjet(Grid g, uint8_t* __restrict__ out, float c0, float c1, f
     }
 }
 
-// staggered sharp on the handle's padded velocity planes (examples/benchmark.jl:61-63)
-__global__ void k_sharp(Grid g, float* __restrict__ vel) {
-    const long long NP = g.NP;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < 3 * NP; c += (long long)gridDim.x * blockDim.x)
-        vel[c] = __fmul_rn(vel[c], g.dinv[c / NP]);
+// staggered sharp on the handle's padded velocity grid (examples/benchmark.jl:61-63)
+__global__ void k_sharp(Grid g, float4* __restrict__ vel) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.NP; c += (long long)gridDim.x * blockDim.x) {
+        float4 v = vel[c];
+        v.x = __fmul_rn(v.x, g.dinv[0]);
+        v.y = __fmul_rn(v.y, g.dinv[1]);
+        v.z = __fmul_rn(v.z, g.dinv[2]);
+        vel[c] = v;
+    }
 }
 
 __device__ __forceinline__ void decode(const Grid& g, long long c, int& x, int& y, int& z) {
@@ -56,43 +60,38 @@ __device__ __forceinline__ void decode(const Grid& g, long long c, int& x, int& 
     z = (int)(r / g.n[1]);
 }
 
-// div! (parallel.jl:131-152) from the velocity planes
-__global__ void k_div(Grid g, const float* __restrict__ vel, float* __restrict__ f) {
-    const float* vx = vel;
-    const float* vy = vel + g.NP;
-    const float* vz = vel + 2 * g.NP;
+// div! (parallel.jl:131-152) from the padded velocity grid
+__global__ void k_div(Grid g, const float4* __restrict__ vel, float* __restrict__ f) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
         int x, y, z;
         decode(g, c, x, y, z);
         const int xm = (x == 0) ? g.n[0] - 1 : x - 1;
         const int ym = (y == 0) ? g.n[1] - 1 : y - 1;
         const int zm = (z == 0) ? g.n[2] - 1 : z - 1;
-        const int p = pcell(g, x, y, z);
-        const float t0 = (vx[p] - vx[pcell(g, xm, y, z)]) * g.inv_d2[0];
-        const float t1 = (vy[p] - vy[pcell(g, x, ym, z)]) * g.inv_d2[1];
-        const float t2 = (vz[p] - vz[pcell(g, x, y, zm)]) * g.inv_d2[2];
+        const float4 v = vel[pcell(g, x, y, z)];
+        const float t0 = (v.x - vel[pcell(g, xm, y, z)].x) * g.inv_d2[0];
+        const float t1 = (v.y - vel[pcell(g, x, ym, z)].y) * g.inv_d2[1];
+        const float t2 = (v.z - vel[pcell(g, x, y, zm)].z) * g.inv_d2[2];
         f[c] = (t0 + t1) + t2;
     }
 }
 
-__global__ void k_vel_to_aos(Grid g, const float* __restrict__ vel, float* __restrict__ aos) {
+__global__ void k_vel_to_aos(Grid g, const float4* __restrict__ vel, float* __restrict__ aos) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
         int x, y, z;
         decode(g, c, x, y, z);
-        const int p = pcell(g, x, y, z);
-        aos[3 * c + 0] = vel[p];
-        aos[3 * c + 1] = vel[g.NP + p];
-        aos[3 * c + 2] = vel[2 * g.NP + p];
+        const float4 v = vel[pcell(g, x, y, z)];
+        aos[3 * c + 0] = v.x;
+        aos[3 * c + 1] = v.y;
+        aos[3 * c + 2] = v.z;
     }
 }
 
-__global__ void k_vel_from_aos(Grid g, const float* __restrict__ aos, float* __restrict__ vel) {
+__global__ void k_vel_from_aos(Grid g, const float* __restrict__ aos, float4* __restrict__ vel) {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
         int x, y, z;
         decode(g, c, x, y, z);
-        pstore(g, vel, x, y, z, aos[3 * c + 0]);
-        pstore(g, vel + g.NP, x, y, z, aos[3 * c + 1]);
-        pstore(g, vel + 2 * g.NP, x, y, z, aos[3 * c + 2]);
+        pstore(g, vel, x, y, z, make_float3(aos[3 * c + 0], aos[3 * c + 1], aos[3 * c + 2]));
     }
 }
 
@@ -135,19 +134,19 @@ cudaError_t launch_isjet(const Grid& g, uint8_t* out, const float* cen, float le
     return cudaGetLastError();
 }
 cudaError_t launch_sharp(const Grid& g, float* vel, cudaStream_t s) {
-    k_sharp<<<grid_for(3 * g.NP, 256), 256, 0, s>>>(g, vel);
+    k_sharp<<<grid_for(g.NP, 256), 256, 0, s>>>(g, reinterpret_cast<float4*>(vel));
     return cudaGetLastError();
 }
 cudaError_t launch_div(const Grid& g, const float* vel, float* f, cudaStream_t s) {
-    k_div<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, f);
+    k_div<<<grid_for(g.N, 256), 256, 0, s>>>(g, reinterpret_cast<const float4*>(vel), f);
     return cudaGetLastError();
 }
 cudaError_t launch_vel_to_aos(const Grid& g, const float* vel, float* aos, cudaStream_t s) {
-    k_vel_to_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, vel, aos);
+    k_vel_to_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, reinterpret_cast<const float4*>(vel), aos);
     return cudaGetLastError();
 }
 cudaError_t launch_vel_from_aos(const Grid& g, const float* aos, float* vel, cudaStream_t s) {
-    k_vel_from_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, aos, vel);
+    k_vel_from_aos<<<grid_for(g.N, 256), 256, 0, s>>>(g, aos, reinterpret_cast<float4*>(vel));
     return cudaGetLastError();
 }
 

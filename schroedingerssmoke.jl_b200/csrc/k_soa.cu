@@ -37,22 +37,20 @@ __global__ void k_psi_to_f64(const float4* __restrict__ psi, double2* __restrict
     }
 }
 
-// padded velocity planes (with their periodic +face copies) <- vx, vy, vz
+// padded velocity grid (with its periodic +face copies) <- vx, vy, vz
 __global__ void k_vel_from_f64(Grid g, const double* __restrict__ vx, const double* __restrict__ vy,
-                               const double* __restrict__ vz, float* __restrict__ vel) {
+                               const double* __restrict__ vz, float4* __restrict__ vel) {
     pdl_enter();
     const int nx = g.n[0], ny = g.n[1];
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.N; c += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(c % nx);
         const long long r = c / nx;
         const int y = (int)(r % ny), z = (int)(r / ny);
-        pstore(g, vel, x, y, z, (float)vx[c]);
-        pstore(g, vel + g.NP, x, y, z, (float)vy[c]);
-        pstore(g, vel + 2 * g.NP, x, y, z, (float)vz[c]);
+        pstore(g, vel, x, y, z, make_float3((float)vx[c], (float)vy[c], (float)vz[c]));
     }
 }
 
-__global__ void k_vel_to_f64(Grid g, const float* __restrict__ vel, double* __restrict__ vx, double* __restrict__ vy,
+__global__ void k_vel_to_f64(Grid g, const float4* __restrict__ vel, double* __restrict__ vx, double* __restrict__ vy,
                              double* __restrict__ vz) {
     pdl_enter();
     const int nx = g.n[0], ny = g.n[1];
@@ -60,10 +58,10 @@ __global__ void k_vel_to_f64(Grid g, const float* __restrict__ vel, double* __re
         const int x = (int)(c % nx);
         const long long r = c / nx;
         const int y = (int)(r % ny), z = (int)(r / ny);
-        const int pc = pcell(g, x, y, z);
-        vx[c] = vel[pc];
-        vy[c] = vel[g.NP + pc];
-        vz[c] = vel[2 * g.NP + pc];
+        const float4 v = vel[pcell(g, x, y, z)];
+        vx[c] = v.x;
+        vy[c] = v.y;
+        vz[c] = v.z;
     }
 }
 
@@ -113,11 +111,12 @@ cudaError_t launch_psi_to_f64(const float* psi, double* a, double* b, long long 
 
 cudaError_t launch_vel_from_f64(const Grid& g, const double* vx, const double* vy, const double* vz, float* vel,
                                 cudaStream_t s) {
-    return launch_pdl(k_vel_from_f64, dim3(blocks(g.N)), dim3(kBlk), 0, s, g, vx, vy, vz, vel);
+    return launch_pdl(k_vel_from_f64, dim3(blocks(g.N)), dim3(kBlk), 0, s, g, vx, vy, vz, reinterpret_cast<float4*>(vel));
 }
 
 cudaError_t launch_vel_to_f64(const Grid& g, const float* vel, double* vx, double* vy, double* vz, cudaStream_t s) {
-    return launch_pdl(k_vel_to_f64, dim3(blocks(g.N)), dim3(kBlk), 0, s, g, vel, vx, vy, vz);
+    return launch_pdl(k_vel_to_f64, dim3(blocks(g.N)), dim3(kBlk), 0, s, g, reinterpret_cast<const float4*>(vel), vx, vy,
+                      vz);
 }
 
 cudaError_t launch_real_from_f64(const double* src, long long stride, double scale, float* dst, long long n,

@@ -10,7 +10,7 @@
 //   ST_DIV  f = div(velocity_one_form(psi, 1))       parallel.jl:100-122, 131-152
 //           with psi optionally restricted in the nozzle on the fly
 //           (restrict_kernel, particles.jl:12-20)
-//   ST_VEL  padded velocity planes vx | vy | vz = one_form(psi, hbar) [* 1/d]
+//   ST_VEL  padded velocity grid (vx, vy, vz, 0) = one_form(psi, hbar) [* 1/d]
 //           (parallel.jl:115-122, staggered sharp examples/benchmark.jl:61-63)
 #include "isf_launch.h"
 
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
     const bool sharp = a.sharp != 0;
     const float di0 = g.dinv[0], di1 = g.dinv[1], di2 = g.dinv[2];
     const int pnx = g.pnx, pnxy = g.pnxy;
-    const int NP = (int)g.NP;
+    float4* __restrict__ out4 = reinterpret_cast<float4*>(out);
     const int ox = nx, oy = ny * pnx, oz = nz * pnxy;  // +face copy offsets
     auto tile_e = [&](int k, int z) -> float4 {
         const int cidx = toff[k] + nxy * z;
@@ -195,15 +195,10 @@ __global__ void __launch_bounds__(BX* TY) k_stencil(StencilArgs a) {
                     }
                     const int y = y0 + r;
                     const int pc = x + pnx * y + pnxy * z;
-                    out[pc] = ax;
-                    out[NP + pc] = ay;
-                    out[2 * NP + pc] = az;
+                    const float4 v = make_float4(ax, ay, az, 0.f);
+                    out4[pc] = v;
                     const bool cx = x == 0, cy = y == 0, cz = z == 0;
-                    if (cx | cy | cz) {  // periodic copies on the +faces
-                        pcopies(out, pc, cx, cy, cz, ox, oy, oz, ax);
-                        pcopies(out + NP, pc, cx, cy, cz, ox, oy, oz, ay);
-                        pcopies(out + 2 * NP, pc, cx, cy, cz, ox, oy, oz, az);
-                    }
+                    if (cx | cy | cz) pcopies(out4, pc, cx, cy, cz, ox, oy, oz, v);  // periodic copies on the +faces
                 }
             }
         }
