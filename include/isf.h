@@ -76,7 +76,7 @@ typedef struct isf_params {
     float dt;                 /* time step */
     int32_t device;           /* CUDA device ordinal */
     int32_t flags;            /* ISF_FLAG_* bits (0: the reference's semantics) */
-    void* stream;             /* cudaStream_t to run on, or NULL: the handle makes its own */
+    void* stream;             /* cudaStream_t to run on (cudaStreamLegacy included), or NULL: the handle makes its own */
 } isf_params;
 
 /* Arguments of one fused time step (the simloop body, examples/benchmark.jl:46-65). */

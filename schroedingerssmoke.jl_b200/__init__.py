@@ -27,8 +27,13 @@ __all__ = [
     "ISF", "ISFBatch", "ISFError", "ParticleLoss", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
     "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
     "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER", "EMIT_RING_PLANE", "FLAG_NORMALIZED_WEIGHTS",
-    "FLAG_CHECK_NAN",
+    "FLAG_CHECK_NAN", "STREAM_LEGACY",
 ]
+
+
+# the CUDA runtime's handle of the legacy default stream (cudaStreamLegacy),
+# the stream torch's default-stream work runs on
+STREAM_LEGACY = 1
 
 
 def _ptr(t: torch.Tensor | None):
@@ -46,7 +51,8 @@ class ISF:
 
     def __init__(self, physical_size, dims, hbar, dt, device: int = 0, flags: int = 0, stream=None):
         # stream: a torch.cuda.Stream for all the handle's work (then without
-        # the separate particle stream), or None for a stream of its own
+        # the separate particle stream), STREAM_LEGACY for the legacy default
+        # stream, or None for a stream of its own
         if not torch.cuda.is_available():
             raise ISFError(_lib.ISF_ERR_CUDA, "no CUDA device: libisf has no CPU path")
         self.L = _lib.load()
@@ -57,7 +63,7 @@ class ISF:
         p.dt = float(dt)
         p.device = int(device)
         p.flags = int(flags)
-        p.stream = None if stream is None else stream.cuda_stream
+        p.stream = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
         h = C.c_void_p()
         check(self.L.isf_create(C.byref(p), C.byref(h)))
         self.h = h
@@ -72,7 +78,8 @@ class ISF:
         self.dt = float(torch.tensor(dt, dtype=torch.float32))
         s = C.c_void_p()
         check(self.L.isf_get_stream(h, C.byref(s)), h)
-        self.stream = torch.cuda.ExternalStream(s.value, device=self.device)
+        self.stream = (torch.cuda.default_stream(self.device) if s.value == STREAM_LEGACY
+                       else torch.cuda.ExternalStream(s.value, device=self.device))
         nx, ny, nz = self.grid_res
         self.shape = (nz, ny, nx)
         self.ncells = nx * ny * nz

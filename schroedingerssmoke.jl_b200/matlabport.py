@@ -15,6 +15,10 @@ Arrays are indexed [x, y, z] as in Julia: a field of an ISF with resolution
 results are CUDA tensors; numpy arrays are copied to the device and the
 results come back as numpy arrays (the reference's Arrays live on the host).
 Slot lists (`Particles.active`, `Keep` indices) are 0-based int64.
+
+Every call runs on the legacy default stream, the one torch's default-stream
+work uses, so the calls are ordered with each other (including the ones
+without an ISF argument) and with the caller's torch operations.
 """
 from __future__ import annotations
 
@@ -56,7 +60,8 @@ class _Grid:
 
     def __init__(self, vol_size, vol_res, hbar, dt, device):
         from . import ISF as _ISF
-        self.isf = _ISF(vol_size, vol_res, hbar, dt, device=device)
+        from . import STREAM_LEGACY
+        self.isf = _ISF(vol_size, vol_res, hbar, dt, device=device, stream=STREAM_LEGACY)
         self.L = self.isf.L
         self.h = self.isf.h
         self.device = self.isf.device

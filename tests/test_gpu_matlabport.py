@@ -47,6 +47,8 @@ def test_fields_match_matlabport_oracle(mp, L, dims):
     obj = mp.ISF(L, dims, HBAR, DT)
     oo = orc_mp.MatlabISF(L, dims, HBAR, DT)
     psi1, psi2 = psi_xyz(dims, 3)
+    # every front-end call runs on the legacy default stream (ordered with the others and with torch)
+    assert obj._g.isf.stream == torch.cuda.default_stream()
 
     a = mp.SchroedingerFlow(obj, psi1, psi2)
     b = orc_mp.schroedinger_flow(oo, psi1, psi2)
