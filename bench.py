@@ -214,6 +214,45 @@ def cpu_baseline(c, psi0, parts0, budget_s, steps_cap=None):
                       f"src/parallel.jl (OpenMP, own FFT; FFTW is absent)"}
 
 
+def oracle_parity(pkg, c, psi0, parts0, local, steps=10, every=16):
+    """The GPU step against the FP64 oracle on the bench workload: `steps`
+    steps from the same initial state; psi's relative L2 error and the largest
+    particle error (as a fraction of the box) over every `every`-th slot, for
+    the particles whose FP64 sample points stayed 1e-4 cells from every face
+    (where FP32 and FP64 may pick different cells).  Part of the CPU leg: the
+    oracle only checks."""
+    import torch
+    import __graft_entry__ as ge
+    oracle = ge.load_oracle()
+    oracle.build()
+    orc = oracle.Oracle(c["L"], c["dims"], c["hbar"], c["dt"], prec=64)
+    psi64 = psi0.astype(np.float64)
+    sub = slice(None, None, every)
+    p64 = parts0[sub].astype(np.float64)
+    margin = np.full(len(p64), 1e30)
+    isf = pkg.ISF(c["L"], c["dims"], c["hbar"], c["dt"], device=local)
+    psi = torch.from_numpy(psi0).to(f"cuda:{local}")
+    parts = torch.from_numpy(parts0).to(f"cuda:{local}")
+    for _ in range(steps):
+        pkg.step(isf, psi, parts, None)
+        m = np.zeros(len(p64))
+        orc.step(psi64, p64, None, margin=m)
+        margin = np.minimum(margin, m)
+    isf.sync()
+    pg = parts.cpu().numpy().astype(np.float64)[sub]
+    g = psi.cpu().numpy().astype(np.float64)
+    psi_err = float(np.linalg.norm(g - psi64) / np.linalg.norm(psi64))
+    both = (pg[:, 0] >= 0) & (p64[:, 0] >= 0)
+    ok = both & (margin > 1e-4)
+    err = np.abs(pg - p64).max(axis=1) / min(c["L"])
+    isf.close()
+    return {"steps": steps, "oracle": "FP64 restatement (oracle/isf_oracle.cpp)", "psi_rel_l2": psi_err,
+            "particles_max_err_of_box": float(err[ok].max()) if ok.any() else None,
+            "particles_checked": int(ok.sum()), "particles_sampled": int(len(p64)),
+            "alive_mismatch": int(((pg[:, 0] >= 0) != (p64[:, 0] >= 0)).sum()),
+            "sample": f"every {every}th particle slot", "bar": 1e-4}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -604,8 +643,10 @@ def main():
         matlab = matlabport_loop(pkg, cfgs, min(args.steps, 200), args.warmup, local)
 
     cb = None
+    parity = None
     if not args.no_cpu:
         cb = cpu_baseline(c, psi0, parts0, args.cpu_seconds)
+        parity = oracle_parity(pkg, c, psi0, parts0, local)
         if matlab is not None:
             matlab["cpu_baseline"] = matlabport_cpu_baseline(cfgs)
 
@@ -625,7 +666,7 @@ def main():
                           "unit": "GB/s", "frac": step_achieved / peak},
         "kernels_ms_per_step": {k: v[0] / args.steps for k, v in sorted(sites.items(), key=lambda kv: -kv[1][0])},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "cpu_baseline": cb,
-        "batched": batched, "batched_sharded": sharded, "adjoint": adjoint, "matlabport": matlab,
+        "batched": batched, "batched_sharded": sharded, "adjoint": adjoint, "matlabport": matlab, "parity": parity,
     }
     print(json.dumps(line), flush=True)
 
