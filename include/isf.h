@@ -147,6 +147,11 @@ ISF_API int isf_isjet(isf_handle* h, uint8_t* jetmask_dev, const float cen[3], f
  * jetmask_dev may be NULL: the nozzle (cen, len, rad) is then evaluated per cell. */
 ISF_API int isf_restrict_velocity(isf_handle* h, float* psi, const float kvec[3], const uint8_t* jetmask_dev,
                           const float cen[3], float len, float rad, float omgterm, int32_t phase_mode);
+/* The jet set-up loop (examples/benchmark.jl:28-31): iters times
+ * restrict_velocity!(isf, psi, kvec, isjetarr, 0) then pressure_project!(isf, psi),
+ * in one call.  jetmask_dev may be NULL: the nozzle is evaluated per cell. */
+ISF_API int isf_init_jet(isf_handle* h, float* psi, int32_t iters, const float kvec[3], const uint8_t* jetmask_dev,
+                         const float cen[3], float len, float rad, int32_t phase_mode);
 /* add_particles!(particles, start:start+count-1, cen, rad)   src/particles.jl:60-94
  * slots wrap modulo nslots; seeded Philox stream (seed, counter). */
 ISF_API int isf_add_particles(isf_handle* h, float* particles, int64_t nslots, int64_t start, int64_t count,

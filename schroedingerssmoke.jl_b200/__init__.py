@@ -25,7 +25,7 @@ from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CH
 
 __all__ = [
     "ISF", "ISFBatch", "ISFError", "ParticleLoss", "schroedinger_flow", "normalize_psi", "pressure_project", "velocity_one_form",
-    "staggered_sharp", "isjet", "restrict_velocity", "add_particles", "staggered_advect", "step", "new_psi",
+    "staggered_sharp", "isjet", "restrict_velocity", "init_jet", "add_particles", "staggered_advect", "step", "new_psi",
     "PHASE_DOT", "PHASE_REFERENCE_SUM", "EMIT_RING", "EMIT_DISC", "EMIT_CYLINDER", "EMIT_RING_PLANE", "FLAG_NORMALIZED_WEIGHTS",
     "FLAG_CHECK_NAN", "STREAM_LEGACY",
 ]
@@ -256,6 +256,19 @@ def restrict_velocity(isf: ISF, psi: torch.Tensor, kvec, isjetarr=None, omgterm:
     cen, ln, rad = nozzle if nozzle is not None else ((0.0, 0.0, 0.0), 0.0, 0.0)
     check(isf.L.isf_restrict_velocity(isf.h, isf._psi(psi), f3(kvec), _ptr(isjetarr), f3(cen), float(ln),
                                       float(rad), float(omgterm), int(phase_mode)), isf.h)
+    return psi
+
+
+def init_jet(isf: ISF, psi: torch.Tensor, iters: int, kvec, isjetarr=None, *, nozzle=None,
+             phase_mode: int = PHASE_REFERENCE_SUM) -> torch.Tensor:
+    """The jet set-up loop of examples/benchmark.jl:28-31 in one library call:
+    `iters` times restrict_velocity!(isf, psi, kvec, isjetarr, 0) followed by
+    pressure_project!(isf, psi)."""
+    if isjetarr is None and nozzle is None:
+        raise ISFError(_lib.ISF_ERR_INVALID, "init_jet needs isjetarr or nozzle")
+    cen, ln, rad = nozzle if nozzle is not None else ((0.0, 0.0, 0.0), 0.0, 0.0)
+    check(isf.L.isf_init_jet(isf.h, isf._psi(psi), int(iters), f3(kvec), _ptr(isjetarr), f3(cen), float(ln),
+                             float(rad), int(phase_mode)), isf.h)
     return psi
 
 

@@ -21,7 +21,7 @@ EXPORTS = (
     "isf_create", "isf_destroy", "isf_last_error", "isf_get_stream", "isf_sync", "isf_join", "isf_malloc", "isf_free",
     "isf_memcpy_h2d", "isf_memcpy_d2h", "isf_grid_info", "isf_schroedinger_flow", "isf_normalize_psi",
     "isf_pressure_project", "isf_velocity_one_form", "isf_staggered_sharp", "isf_get_velocity",
-    "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_add_particles", "isf_staggered_advect",
+    "isf_set_velocity", "isf_isjet", "isf_restrict_velocity", "isf_init_jet", "isf_add_particles", "isf_staggered_advect",
     "isf_step", "isf_div", "isf_poisson_solve", "isf_fft3", "isf_counters", "isf_counters_async", "isf_profile_start",
     "isf_profile_stop", "isf_profile_sites", "isf_profile_get", "isf_launch_count", "isf_poisson_solve_static",
     "isf_static_last_error", "isf_batch_create", "isf_batch_destroy", "isf_batch_last_error",
@@ -146,6 +146,7 @@ def load(path: str | None = None):
         "isf_set_velocity": [vp, vp],
         "isf_isjet": [vp, vp, fp, f32, f32],
         "isf_restrict_velocity": [vp, vp, fp, vp, fp, f32, f32, f32, i32],
+        "isf_init_jet": [vp, vp, i32, fp, vp, fp, f32, f32, i32],
         "isf_add_particles": [vp, vp, i64, i64, i64, fp, f32, f32, u64, u64, i32],
         "isf_staggered_advect": [vp, vp, i64],
         "isf_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs)],

@@ -545,6 +545,22 @@ int isf_restrict_velocity(isf_handle* h, float* psi, const float kvec[3], const 
     return ISF_OK;
 }
 
+int isf_init_jet(isf_handle* h, float* psi, int32_t iters, const float kvec[3], const uint8_t* mask, const float cen[3],
+                 float len, float rad, int32_t phase_mode) {
+    ISF_ENTER(h);
+    if (!psi || !kvec || (!mask && !cen) || iters < 0) return fail(h, ISF_ERR_INVALID, "isf_init_jet: bad argument");
+    ISF_ALIGNED(h, psi, 16, "psi");
+    if (phase_mode != ISF_PHASE_REFERENCE_SUM && phase_mode != ISF_PHASE_DOT)
+        return fail(h, ISF_ERR_INVALID, "isf_init_jet: bad phase_mode");
+    const float zero[3] = {0.f, 0.f, 0.f};
+    // restrict_velocity!(isf, psi, kvec, isjet, 0) + pressure_project!, the
+    // restriction fused into the projection's stencil and gauge pass as in isf_step
+    JetArgs j = make_jet(kvec, mask, cen ? cen : zero, len, rad, 0.f, phase_mode);
+    for (int it = 0; it < iters; ++it)
+        if (int rc = run_projection(h, psi, &j)) return rc;
+    return ISF_OK;
+}
+
 int isf_add_particles(isf_handle* h, float* parts, int64_t nslots, int64_t start, int64_t count, const float cen[3],
                       float len, float rad, uint64_t seed, uint64_t counter, int32_t mode) {
     ISF_ENTER(h);

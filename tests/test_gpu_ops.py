@@ -369,3 +369,32 @@ def test_particle_stream_matches_single_stream(isfpkg, cfgs):
     assert torch.equal(vel_a, vel_b)
     assert torch.equal(res["two"], res["one"])
     assert int(res["two"][-1, 1]) > 20000
+
+
+@pytest.mark.parametrize("phase_mode", [0, 1])
+def test_init_jet_matches_loop_and_oracle(isfpkg, oracle_mod, cfgs, phase_mode):
+    """isf_init_jet (the jet set-up loop in one call, restriction fused into
+    the projection) against the same loop of restrict_velocity + pressure_project
+    through the API, and against the FP64 oracle."""
+    L, dims = (4, 2, 2), (64, 32, 32)
+    noz = cfgs.JET_NOZZLE
+    kvec, _ = cfgs.jet_omega()
+    isf = isfpkg.ISF(L, dims, HBAR, DT)
+    psi0 = cfgs.jet_init_psi(dims)
+    a = cuda(psi0)
+    isfpkg.init_jet(isf, a, 10, kvec, nozzle=(noz["cen"], noz["len"], noz["rad"]), phase_mode=phase_mode)
+    b = cuda(psi0)
+    for _ in range(10):
+        isfpkg.restrict_velocity(isf, b, kvec, None, 0.0, nozzle=(noz["cen"], noz["len"], noz["rad"]),
+                                 phase_mode=phase_mode)
+        isfpkg.pressure_project(isf, b)
+    isf.sync()
+    assert rel(host(a), host(b)) < 1e-6
+    orc = oracle_mod.Oracle(L, dims, HBAR, DT)
+    psi64 = psi0.copy()
+    for _ in range(10):
+        orc.restrict_velocity(psi64, kvec, 0.0, noz["cen"], noz["len"], noz["rad"], phase_mode=phase_mode)
+        orc.pressure_project(psi64)
+    assert rel(host(a), psi64) < 2e-5
+    with pytest.raises(Exception):
+        isfpkg.init_jet(isf, a, -1, kvec, nozzle=(noz["cen"], noz["len"], noz["rad"]))
