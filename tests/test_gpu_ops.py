@@ -398,3 +398,26 @@ def test_init_jet_matches_loop_and_oracle(isfpkg, oracle_mod, cfgs, phase_mode):
     assert rel(host(a), psi64) < 2e-5
     with pytest.raises(Exception):
         isfpkg.init_jet(isf, a, -1, kvec, nozzle=(noz["cen"], noz["len"], noz["rad"]))
+
+
+def test_step_without_particles_both_stream_kinds(isfpkg, cfgs):
+    """isf_step with no particle slots queues no particle work: a handle with
+    its own streams and one on a caller stream give the same psi bits, and a
+    later call with particles still orders correctly after it."""
+    L, dims = (4, 2, 2), (64, 32, 32)
+    psi0 = cuda(smooth_psi(dims, seed=4))
+    own = isfpkg.ISF(L, dims, HBAR, DT)
+    caller = isfpkg.ISF(L, dims, HBAR, DT, stream=torch.cuda.Stream())
+    out = []
+    for isf in (own, caller):
+        psi = psi0.clone()
+        torch.cuda.synchronize()
+        for _ in range(3):
+            isfpkg.step(isf, psi, None, None)
+        parts = cuda(np.random.default_rng(2).uniform(0.2, 0.8, (1000, 3)) * np.asarray(L))
+        torch.cuda.synchronize()
+        isfpkg.step(isf, psi, parts, None)
+        isf.sync()
+        out.append((psi, parts))
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
