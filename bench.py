@@ -246,11 +246,19 @@ def oracle_parity(pkg, c, psi0, parts0, local, steps=10, every=16):
     ok = both & (margin > 1e-4)
     err = np.abs(pg - p64).max(axis=1) / min(c["L"])
     isf.close()
-    return {"steps": steps, "oracle": "FP64 restatement (oracle/isf_oracle.cpp)", "psi_rel_l2": psi_err,
-            "particles_max_err_of_box": float(err[ok].max()) if ok.any() else None,
-            "particles_checked": int(ok.sum()), "particles_sampled": int(len(p64)),
-            "alive_mismatch": int(((pg[:, 0] >= 0) != (p64[:, 0] >= 0)).sum()),
-            "sample": f"every {every}th particle slot", "bar": 1e-4}
+    bar = 1e-4
+    perr = float(err[ok].max()) if ok.any() else None
+    mismatch = int(((pg[:, 0] >= 0) != (p64[:, 0] >= 0)).sum())
+    # every error against the bar; alive/dead disagreements as a fraction of the sampled slots
+    within = {"psi": psi_err <= bar, "particles": perr is not None and perr <= bar,
+              "alive": mismatch <= bar * len(p64)}
+    res = {"steps": steps, "oracle": "FP64 restatement (oracle/isf_oracle.cpp)", "psi_rel_l2": psi_err,
+           "particles_max_err_of_box": perr, "particles_checked": int(ok.sum()), "particles_sampled": int(len(p64)),
+           "alive_mismatch": mismatch, "sample": f"every {every}th particle slot", "bar": bar,
+           "within_bar": within, "ok": all(within.values())}
+    if not res["ok"]:
+        print(f"bench: PARITY FAILURE against the FP64 oracle: {json.dumps(res)}", file=sys.stderr, flush=True)
+    return res
 
 
 def run_reference(args):

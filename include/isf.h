@@ -197,7 +197,11 @@ ISF_API int isf_counters_async(isf_handle* h, uint64_t* host_out, int32_t n, int
  * legacy default stream) of params->device; f and q are device arrays of N
  * floats.  All calls share the workspace: calls that overlap on the GPU race,
  * so serialise them.  The first call on a device looks up the workspace
- * address; make it before any stream capture.  Errors: isf_static_last_error(). */
+ * address; make it before any stream capture.  The grid tables are uploaded
+ * from host memory when (grid_res, physical_size, hbar, dt) differ from the
+ * previous call's on that device; a call that needs such an upload while
+ * params->stream is being captured returns ISF_ERR_INVALID and queues
+ * nothing.  Errors: isf_static_last_error(). */
 ISF_API int isf_poisson_solve_static(const isf_params* params, const float* f_dev, float* q_dev);
 ISF_API const char* isf_static_last_error(void);
 

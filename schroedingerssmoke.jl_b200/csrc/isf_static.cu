@@ -19,6 +19,13 @@
 // on the shared arrays; serialise them.  The first call on a device looks up
 // the arrays' device addresses (cudaGetSymbolAddress, once per device, with
 // that device current); make that first call before any stream capture.
+//
+// The tables depend only on the grid parameters (grid_res, physical_size,
+// hbar, dt).  A call uploads them from host memory when they differ from the
+// last upload on that device and skips the upload otherwise.  An upload is a
+// copy from a host buffer that lives only during the call, so a call that
+// needs one while its stream is being captured is refused (ISF_ERR_INVALID)
+// before anything is queued.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -41,6 +48,10 @@ struct StaticAddrs {
     float2* spectrum = nullptr;
     char* tables = nullptr;
     bool ready = false;
+    // grid parameters of the tables last uploaded to this device
+    bool have_key = false;
+    int key_n[3] = {0, 0, 0}, key_L[3] = {0, 0, 0};
+    float key_hbar = 0.f, key_dt = 0.f;
 };
 constexpr int kMaxDevices = 64;
 StaticAddrs g_addrs[kMaxDevices];
@@ -71,6 +82,25 @@ cudaError_t static_addrs(int dev, StaticAddrs& out) {
     }
     out = a;
     return cudaSuccess;
+}
+
+bool same_key(const StaticAddrs& a, const isf_params* p) {
+    if (!a.have_key) return false;
+    for (int k = 0; k < 3; ++k)
+        if (a.key_n[k] != p->grid_res[k] || a.key_L[k] != p->physical_size[k]) return false;
+    return std::memcmp(&a.key_hbar, &p->hbar, sizeof(float)) == 0 && std::memcmp(&a.key_dt, &p->dt, sizeof(float)) == 0;
+}
+
+void set_key(int dev, const isf_params* p) {
+    std::lock_guard<std::mutex> lock(g_addrs_mutex);
+    StaticAddrs& a = g_addrs[dev];
+    for (int k = 0; k < 3; ++k) {
+        a.key_n[k] = p->grid_res[k];
+        a.key_L[k] = p->physical_size[k];
+    }
+    a.key_hbar = p->hbar;
+    a.key_dt = p->dt;
+    a.have_key = true;
 }
 
 }  // namespace
@@ -111,9 +141,22 @@ int isf_poisson_solve_static(const isf_params* p, const float* f, float* q) {
     std::vector<char> host;
     fill_grid(p->grid_res, p->physical_size, p->hbar, p->dt, g, host);
     cudaStream_t s = (cudaStream_t)p->stream;
-    // pageable source: the copy is staged before cudaMemcpyAsync returns
-    if ((e = cudaMemcpyAsync(addrs.tables, host.data(), host.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-        return finish(ISF_ERR_CUDA, std::string("isf_poisson_solve_static: table upload: ") + cudaGetErrorString(e));
+    if (!same_key(addrs, p)) {
+        // a new upload: refused under stream capture, which would record a
+        // copy from this call's host buffer (freed when the call returns)
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        e = cudaStreamIsCapturing(s, &cap);
+        if (e != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+            if (e != cudaSuccess) cudaGetLastError();
+            return finish(ISF_ERR_INVALID,
+                          "isf_poisson_solve_static: new grid parameters need a table upload, which cannot be made "
+                          "while the stream is being captured; make one call with these parameters first");
+        }
+        // pageable source: the copy is staged before cudaMemcpyAsync returns
+        if ((e = cudaMemcpyAsync(addrs.tables, host.data(), host.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return finish(ISF_ERR_CUDA, std::string("isf_poisson_solve_static: table upload: ") + cudaGetErrorString(e));
+        set_key(p->device, p);
+    }
     bind_tables(g, addrs.tables);
 
     XArgs xa;

@@ -66,3 +66,33 @@ def test_static_poisson_rejects_grids_beyond_the_workspace(isfpkg):
     rc = lib.isf_poisson_solve_static(C.byref(p), C.c_void_p(dummy.data_ptr()), C.c_void_p(dummy.data_ptr()))
     assert rc == _lib.ISF_ERR_INVALID
     assert b"static workspace" in lib.isf_static_last_error()
+
+
+def test_static_poisson_refuses_a_table_upload_under_capture(isfpkg):
+    """A call whose grid parameters differ from the previous call's must
+    upload tables from a host buffer that lives only during the call; under
+    stream capture that copy would replay from freed memory, so the call is
+    refused before it queues anything."""
+    import warnings
+
+    _lib = importlib.import_module(isfpkg.__name__ + "._lib")
+    lib = _lib.load()
+    L, dims = (4, 2, 2), (64, 32, 32)
+    f = torch.zeros(dims[::-1], dtype=torch.float32, device="cuda")
+    q = torch.empty_like(f)
+    p = _params(_lib, L, dims)
+    # an ordinary call first: looks up the workspace address and uploads the tables
+    assert lib.isf_poisson_solve_static(C.byref(p), C.c_void_p(f.data_ptr()), C.c_void_p(q.data_ptr())) == 0
+    torch.cuda.synchronize()
+    other = _params(_lib, (2, 2, 2), (32, 32, 32))
+    s = torch.cuda.Stream()
+    other.stream = C.c_void_p(s.cuda_stream)
+    graph = torch.cuda.CUDAGraph()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        with torch.cuda.graph(graph, stream=s):
+            rc = lib.isf_poisson_solve_static(C.byref(other), C.c_void_p(f.data_ptr()), C.c_void_p(q.data_ptr()))
+    del graph
+    assert rc == _lib.ISF_ERR_INVALID
+    assert b"captured" in lib.isf_static_last_error()
+    torch.cuda.synchronize()
