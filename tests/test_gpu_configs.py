@@ -31,37 +31,6 @@ def particle_errors(gpu, ref, margin, L):
     return (err[both].max() if both.any() else 0.0), int((alive_g != alive_r).sum()), int(both.sum())
 
 
-def jet_run(isfpkg, oracle_mod, cfgs, L, dims, steps, slots, emit_per_step, emit_mode, seed, init_particles=None):
-    hbar, dt = cfgs.HBAR, float(np.float32(1 / 48))
-    kvec, omega = cfgs.jet_omega(hbar)
-    noz = cfgs.JET_NOZZLE
-    isf = isfpkg.ISF(L, dims, hbar, dt)
-    orc = oracle_mod.Oracle(L, dims, hbar, dt)
-    psi64 = cfgs.jet_init_psi(dims)
-    psi = cuda(psi64)
-    # jet initialisation: 10 x (restrict, project) (examples/benchmark.jl:28-31)
-    for _ in range(10):
-        isfpkg.restrict_velocity(isf, psi, kvec, None, 0.0, nozzle=(noz["cen"], noz["len"], noz["rad"]),
-                                 phase_mode=isfpkg.PHASE_DOT)
-        isfpkg.pressure_project(isf, psi)
-        orc.restrict_velocity(psi64, kvec, 0.0, noz["cen"], noz["len"], noz["rad"], phase_mode=oracle_mod.PHASE_DOT)
-        orc.pressure_project(psi64)
-    parts64 = np.full((slots, 3), -1.0) if init_particles is None else init_particles.copy()
-    parts = cuda(parts64)
-    margin_min = np.full(slots, 1e30)
-    for it in range(1, steps + 1):
-        t = np.float32(it) * np.float32(dt)
-        jet = dict(kvec=kvec, omega_t=float(np.float32(omega) * t), cen=noz["cen"], len=noz["len"], rad=noz["rad"],
-                   emit_start=((it - 1) * emit_per_step) % slots, emit_count=emit_per_step, seed=seed, counter=it,
-                   emit_mode=emit_mode, phase_mode=isfpkg.PHASE_DOT)
-        isfpkg.step(isf, psi, parts, jet)
-        m = np.zeros(slots)
-        orc.step(psi64, parts64, jet, margin=m)
-        margin_min = np.minimum(margin_min, m)
-    isf.sync()
-    return host(psi), psi64, host(parts), parts64, margin_min
-
-
 def kinetic_energy(psi, L, hbar):
     """hbar^2/2 * sum |k|^2 |psi_hat|^2 / N^2 over both components."""
     nz, ny, nx = psi.shape[:3]
@@ -151,25 +120,107 @@ def test_jet_64x32x32_100_steps(isfpkg, oracle_mod, cfgs):
     print(f"one-step map worst: psi {worst_map[0]:.2e} particles {worst_map[1]:.2e} (step {worst_map[2]})")
 
 
-def test_jet_128x64x64_nozzle_seeded(isfpkg, oracle_mod, cfgs):
+def test_jet_128x64x64_200_steps(isfpkg, oracle_mod, cfgs):
     """The jet at 128x64x64 with 2^20 particles seeded uniformly in the nozzle
-    cylinder (seed 1), 20 steps."""
+    cylinder (seed 1), 200 steps, against an FP64 oracle run of the same steps.
+    The oracle advects every 8th particle (particles do not interact, so the
+    subset sees the same velocity field).
+
+    The flow is chaotic at this resolution.  The FP32 restatement of the
+    reference's arithmetic stays within 1e-4 of the FP64 trajectory up to
+    about step 30 (relative psi distance 5.6e-7 at step 20, 2.4e-5 at 30,
+    6.6e-3 at 40, 0.63 at 200), and the FP64 oracle itself leaves its own
+    trajectory just as fast under a 1e-6 perturbation of psi0.  So the 1e-4
+    bar is held in three ways:
+      * steps 1-30, free-running against the FP64 oracle;
+      * steps 31-200, as a one-step map: every step a second FP64 oracle is
+        reset to the GPU's state and both take the same step;
+      * at step 200, statistics of the free-running GPU run (mean and spread
+        of the particle cloud, the live count, the kinetic energy of psi)
+        against the free-running FP32 restatement.  Runs of the restatement
+        and of the oracle that differ only by rounding-level perturbations of
+        psi0 spread by up to 0.25 in a mean coordinate, 0.23 in a spread,
+        0.9 % in the live count and 9 % in energy at step 200; the tolerances
+        are about twice that.
+    The free-running GPU error against the FP64 oracle at step 200 is printed."""
     L, dims = (4, 2, 2), (128, 64, 64)
     hbar, dt = cfgs.HBAR, float(np.float32(1 / 48))
-    orc = oracle_mod.Oracle(L, dims, hbar, dt)
+    kvec, omega = cfgs.jet_omega(hbar)
     noz = cfgs.JET_NOZZLE
-    P = 1 << 20
-    p0 = np.full((P, 3), -1.0)
-    orc.add_particles(p0, 0, P, noz["cen"], noz["rad"], seed=1, counter=0, mode=oracle_mod.EMIT_CYLINDER,
+    P, every, horizon, steps = 1 << 20, 8, 30, 200
+    isf = isfpkg.ISF(L, dims, hbar, dt)
+    o64 = oracle_mod.Oracle(L, dims, hbar, dt)            # free-running FP64
+    omap = oracle_mod.Oracle(L, dims, hbar, dt)           # one-step map from the GPU state
+    o32 = oracle_mod.Oracle(L, dims, hbar, dt, prec=32)   # free-running FP32 restatement
+    pall = np.full((P, 3), -1.0)
+    o64.add_particles(pall, 0, P, noz["cen"], noz["rad"], seed=1, counter=0, mode=oracle_mod.EMIT_CYLINDER,
                       length=noz["len"])
-    p0 = p0.astype(np.float32).astype(np.float64)
-    g, r, pg, pr, margin = jet_run(isfpkg, oracle_mod, cfgs, L, dims, steps=20, slots=P, emit_per_step=0,
-                                   emit_mode=isfpkg.EMIT_DISC, seed=1, init_particles=p0)
-    assert rel(g, r) < 1e-4
-    perr, mismatch, n = particle_errors(pg, pr, margin, L)
-    assert n > 0.9 * P
-    assert perr < 1e-4, perr
-    assert mismatch <= 1e-3 * P
+    pall = pall.astype(np.float32).astype(np.float64)
+    sub = slice(None, None, every)
+    psi64 = cfgs.jet_init_psi(dims)
+    psi32 = psi64.astype(np.float32)
+    psi = cuda(psi64)
+    for _ in range(10):
+        isfpkg.restrict_velocity(isf, psi, kvec, None, 0.0, nozzle=(noz["cen"], noz["len"], noz["rad"]),
+                                 phase_mode=isfpkg.PHASE_DOT)
+        isfpkg.pressure_project(isf, psi)
+        for o, a in ((o64, psi64), (o32, psi32)):
+            o.restrict_velocity(a, kvec, 0.0, noz["cen"], noz["len"], noz["rad"], phase_mode=oracle_mod.PHASE_DOT)
+            o.pressure_project(a)
+    parts = cuda(pall)
+    p64 = pall[sub].copy()
+    p32 = p64.astype(np.float32)
+    n = len(p64)
+    margin_min = np.full(n, 1e30)
+    worst_map = (0.0, 0.0, 0)
+    for it in range(1, steps + 1):
+        t = np.float32(it) * np.float32(dt)
+        jet = dict(kvec=kvec, omega_t=float(np.float32(omega) * t), cen=noz["cen"], len=noz["len"], rad=noz["rad"],
+                   emit_start=0, emit_count=0, seed=1, counter=it, emit_mode=isfpkg.EMIT_DISC,
+                   phase_mode=isfpkg.PHASE_DOT)
+        if it > horizon:
+            isf.sync()
+            mpsi, mp = host(psi), host(parts)[sub]
+        isfpkg.step(isf, psi, parts, jet)
+        m = np.zeros(n)
+        o64.step(psi64, p64, jet, margin=m)
+        o32.step(psi32, p32, jet)
+        if it <= horizon:
+            margin_min = np.minimum(margin_min, m)
+        if it == horizon:
+            isf.sync()
+            e = rel(host(psi), psi64)
+            perr, mismatch, ok = particle_errors(host(parts)[sub], p64, margin_min, L)
+            assert e < 1e-4, (it, e)
+            assert perr < 1e-4, (it, perr)
+            assert mismatch <= 1e-3 * n, (it, mismatch)
+            assert ok > 0.9 * n, (it, ok)
+            print(f"C2 free-running at step {it}: psi {e:.2e} particles {perr:.2e} ({ok} checked)")
+        if it > horizon:
+            mm = np.zeros(n)
+            omap.step(mpsi, mp, jet, margin=mm)
+            isf.sync()
+            e = rel(host(psi), mpsi)
+            perr, mismatch, ok = particle_errors(host(parts)[sub], mp, mm, L)
+            assert e < 1e-4, (it, e)
+            assert perr < 1e-4, (it, perr)
+            assert mismatch <= 1e-3 * n, (it, mismatch)
+            worst_map = max(worst_map, (e, perr, it))
+    g, pg = host(psi), host(parts)[sub]
+    both = (pg[:, 0] >= 0) & (p64[:, 0] >= 0)
+    free_psi = rel(g, psi64)
+    free_part = float((np.abs(pg[both] - p64[both]).max(axis=1) / min(L)).max())
+    r32 = p32.astype(np.float64)
+    alive_g, alive_r = pg[:, 0] >= 0, r32[:, 0] >= 0
+    assert abs(int(alive_g.sum()) - int(alive_r.sum())) <= 0.02 * n
+    assert np.all(np.abs(pg[alive_g].mean(0) - r32[alive_r].mean(0)) < 0.5)
+    assert np.all(np.abs(pg[alive_g].std(0) - r32[alive_r].std(0)) < 0.45)
+    eg, er = kinetic_energy(g, L, hbar), kinetic_energy(psi32.astype(np.float64), L, hbar)
+    assert abs(eg / er - 1) < 0.2, (eg, er)
+    print(f"C2 one-step map worst: psi {worst_map[0]:.2e} particles {worst_map[1]:.2e} (step {worst_map[2]}); "
+          f"free-running at step {steps}: psi {free_psi:.2e}, particles {free_part:.2e} of the box; "
+          f"step-{steps} statistics GPU/FP32: mean {pg[alive_g].mean(0).round(3)} / {r32[alive_r].mean(0).round(3)}, "
+          f"energy {eg:.4f} / {er:.4f}")
 
 
 @pytest.mark.slow
