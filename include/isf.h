@@ -162,6 +162,26 @@ ISF_API int isf_staggered_advect(isf_handle* h, float* particles, int64_t nparti
 /* One fused time step: the simloop body examples/benchmark.jl:46-65. */
 ISF_API int isf_step(isf_handle* h, float* psi, float* particles, int64_t nparticles, const isf_step_args* args);
 
+/* Cell-sorted traversal of the particle slots.  staggered_advect!
+ * (src/parallel.jl:248-261) advects every slot of the buffer in storage
+ * order, dead ones included.  With every > 0, isf_step advects through a
+ * permutation of the slots instead: live particles grouped by 2 x 2 x 2 cell
+ * tile, so a warp's velocity gathers share cells, and dead slots last, so
+ * they share warps.  Slots never move (a slot stays a particle's identity)
+ * and each particle's arithmetic is unchanged, so the positions are bitwise
+ * those of storage order.  The permutation is rebuilt every `every` steps on
+ * the particle stream (launch sites "step order count / scan / scatter"),
+ * and whenever the slot array or its length changes; particles emitted in
+ * between keep their slot's place in it.  every = 0 restores storage order. */
+ISF_API int isf_set_particle_order(isf_handle* h, int32_t every);
+/* Build the permutation of np slots now, on the handle's stream; the next
+ * isf_step with these particles uses it if ordering is on. */
+ISF_API int isf_sort_particles(isf_handle* h, const float* particles, int64_t nparticles);
+/* *n = the length of the current permutation (0: none); with order non-NULL,
+ * copies it into that device buffer (cap entries), stream-ordered on the
+ * handle's stream. */
+ISF_API int isf_get_particle_order(isf_handle* h, int32_t* order, int64_t cap, int64_t* n);
+
 /* ---- diagnostics (internal stages of the reference, exposed for parity checks) */
 
 /* isf.f from the handle's velocity: div!(isf)   src/parallel.jl:144-152 */

@@ -167,6 +167,27 @@ class ISF:
         check(self.L.isf_launch_count(self.h, C.byref(out)), self.h)
         return int(out.value)
 
+    def set_particle_order(self, every: int):
+        """isf_step advects through a cell-sorted permutation of the slots,
+        rebuilt every `every` steps (0: storage order).  Positions are bitwise
+        the same either way."""
+        check(self.L.isf_set_particle_order(self.h, int(every)), self.h)
+
+    def sort_particles(self, particles: torch.Tensor):
+        ptr, P = self._parts(particles)
+        check(self.L.isf_sort_particles(self.h, ptr, P), self.h)
+
+    def particle_order(self) -> torch.Tensor | None:
+        """The current permutation of the slots (int32, on the device), or None."""
+        n = C.c_int64()
+        check(self.L.isf_get_particle_order(self.h, None, 0, C.byref(n)), self.h)
+        if n.value == 0:
+            return None
+        out = torch.empty(n.value, dtype=torch.int32, device=self.device)
+        check(self.L.isf_get_particle_order(self.h, _ptr(out), n.value, C.byref(n)), self.h)
+        self.sync()
+        return out
+
     def profile_start(self):
         check(self.L.isf_profile_start(self.h), self.h)
 

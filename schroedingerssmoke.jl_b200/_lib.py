@@ -34,6 +34,7 @@ EXPORTS = (
     "isf_psi_from_f64", "isf_psi_to_f64", "isf_velocity_from_f64", "isf_velocity_to_f64", "isf_real_from_f64",
     "isf_real_to_f64", "isf_complex_to_f64", "isf_gauge_transform", "isf_add_particles_soa",
     "isf_staggered_velocity", "isf_advect_active", "isf_keep_inside", "isf_gather_particles",
+    "isf_set_particle_order", "isf_sort_particles", "isf_get_particle_order",
 )
 TILE_KINDS = ("x_psi", "x_real", "y_psi", "z_psi", "y_half", "z_half")
 
@@ -150,6 +151,9 @@ def load(path: str | None = None):
         "isf_add_particles": [vp, vp, i64, i64, i64, fp, f32, f32, u64, u64, i32],
         "isf_staggered_advect": [vp, vp, i64],
         "isf_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs)],
+        "isf_set_particle_order": [vp, i32],
+        "isf_sort_particles": [vp, vp, i64],
+        "isf_get_particle_order": [vp, vp, i64, C.POINTER(i64)],
         "isf_div": [vp, vp],
         "isf_poisson_solve": [vp, vp, vp],
         "isf_fft3": [vp, vp, i32],

@@ -301,6 +301,47 @@ int run_poisson_spectral(isf_handle* h, const char* site) {
     return ISF_OK;
 }
 
+void free_order(isf_handle* h) {
+    cudaFree(h->ord.hist);
+    cudaFree(h->ord.rank);
+    cudaFree(h->ord.sums);
+    cudaFree(h->ord.total);
+    cudaFree(h->ord.order);
+    h->ord = OrderBufs{};
+    h->ord_cap = 0;
+    h->order_n = 0;
+}
+
+// buffers of the cell order for np slots (allocated on first use, grown as needed)
+int ensure_order(isf_handle* h, long long np) {
+    if (h->ord.hist && h->ord_cap >= np) return ISF_OK;
+    free_order(h);
+    const long long cap = np > 0 ? np : 1;
+    if (cudaMalloc(&h->ord.hist, sizeof(unsigned) * order_keys(h->g)) != cudaSuccess ||
+        cudaMalloc(&h->ord.sums, sizeof(unsigned) * order_sums(h->g)) != cudaSuccess ||
+        cudaMalloc(&h->ord.total, sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&h->ord.rank, sizeof(unsigned) * cap) != cudaSuccess ||
+        cudaMalloc(&h->ord.order, sizeof(int) * cap) != cudaSuccess) {
+        cudaGetLastError();
+        free_order(h);
+        return fail(h, ISF_ERR_NOMEM, "particle order: device allocation failed");
+    }
+    h->ord_cap = cap;
+    return ISF_OK;
+}
+
+int run_order(isf_handle* h, const float* parts, long long np, cudaStream_t st, const char* site) {
+    const std::string s(site);
+    ISF_LAUNCH_ON(h, st, launch_order_count(h->g, parts, np, h->ord, st), (s + " order count").c_str());
+    ISF_LAUNCH_ON(h, st, launch_order_scan(h->g, h->ord, st), (s + " order scan").c_str());
+    h->launches += 2;  // the scan is three kernels
+    ISF_LAUNCH_ON(h, st, launch_order_scatter(h->g, parts, np, h->ord, st), (s + " order scatter").c_str());
+    h->order_n = np;
+    h->order_parts = parts;
+    h->order_age = 0;
+    return ISF_OK;
+}
+
 JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], float len, float rad, float omgterm,
                  int mode) {
     JetArgs j;
@@ -405,6 +446,7 @@ int isf_destroy(isf_handle* h) {
         cudaFree(h->tables);
         cudaFree(h->counters);
         cudaFree(h->keep_counts);
+        free_order(h);
         adj_free(h);
         destroy_side(h);
         if (h->own_stream) cudaStreamDestroy(h->stream);
@@ -587,6 +629,33 @@ int isf_staggered_advect(isf_handle* h, float* parts, int64_t np) {
     return ISF_OK;
 }
 
+int isf_set_particle_order(isf_handle* h, int32_t every) {
+    ISF_ENTER(h);
+    if (every < 0) return fail(h, ISF_ERR_INVALID, "isf_set_particle_order: every must be >= 0");
+    h->order_every = every;
+    if (every == 0) h->order_n = 0;
+    return ISF_OK;
+}
+
+int isf_sort_particles(isf_handle* h, const float* parts, int64_t np) {
+    ISF_ENTER(h);
+    if (np <= 0 || !parts) return fail(h, ISF_ERR_INVALID, "isf_sort_particles: bad particles");
+    if (np > kMaxParticles) return fail(h, ISF_ERR_INVALID, "isf_sort_particles: more than 715827882 particles");
+    if (int rc = ensure_order(h, np)) return rc;
+    return run_order(h, parts, np, h->stream, "sort");
+}
+
+int isf_get_particle_order(isf_handle* h, int32_t* order, int64_t cap, int64_t* n) {
+    ISF_ENTER(h);
+    if (!n) return fail(h, ISF_ERR_INVALID, "isf_get_particle_order: null count");
+    *n = h->order_n;
+    if (h->order_n == 0 || !order) return ISF_OK;  // no permutation, or only its length asked for
+    if (cap < h->order_n) return fail(h, ISF_ERR_INVALID, "isf_get_particle_order: buffer too small");
+    ISF_CUDA(h, cudaMemcpyAsync(order, h->ord.order, sizeof(int) * h->order_n, cudaMemcpyDeviceToDevice, h->stream),
+             "isf_get_particle_order");
+    return ISF_OK;
+}
+
 int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step_args* a) {
     ISF_ENTER_NOJOIN(h);
     if (!psi || !a) return fail(h, ISF_ERR_INVALID, "isf_step: null argument");
@@ -601,6 +670,12 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
         if (a->emit_count > 0 && (a->emit_mode < ISF_EMIT_RING || a->emit_mode > ISF_EMIT_RING_PLANE))
             return fail(h, ISF_ERR_INVALID, "isf_step: bad emit_mode");
     }
+    // the cell order of the slots: re-sorted every order_every steps, and
+    // whenever the slot array or its length changes
+    const bool resort = h->order_every > 0 && np > 0 &&
+                        (h->order_n != np || h->order_parts != parts || h->order_age >= h->order_every);
+    if (resort)
+        if (int rc = ensure_order(h, np)) return rc;
     int rc = run_schroedinger(h, psi, true);  // schroedinger_flow! + normalize_psi
     if (rc) return rc;
     rc = run_projection(h, psi, nullptr);     // pressure_project!
@@ -635,7 +710,15 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
         e.mode = a->emit_mode;
         ISF_LAUNCH_ON(h, ps, launch_emit(parts, np, a->emit_start % np, a->emit_count, e, ps), "step emit");
     }
-    if (np > 0) ISF_LAUNCH_ON(h, ps, launch_advect(h->g, parts, np, h->vel, h->counters, ps), "step advect");
+    const int* order = nullptr;
+    if (h->order_every > 0 && np > 0) {
+        if (resort)
+            if (int rc_o = run_order(h, parts, np, ps, "step")) return rc_o;
+        ++h->order_age;
+        order = h->ord.order;
+    }
+    if (np > 0)
+        ISF_LAUNCH_ON(h, ps, launch_advect(h->g, parts, np, h->vel, h->counters, ps, 1, 0, order), "step advect");
     if (h->side && (emit || np > 0)) {
         ISF_CUDA(h, cudaEventRecord(h->ev_read[h->vcur], h->side), "step particle event");
         ISF_CUDA(h, cudaEventRecord(h->ev_side, h->side), "step particle event");

@@ -49,6 +49,13 @@ struct isf_handle {
     std::vector<double> site_ms;
     std::vector<long long> site_count;
     isf_adj_state* adj = nullptr;
+    // cell order of the particle slots (isf_set_particle_order / isf_sort_particles)
+    int order_every = 0;                 // isf_step re-sorts every order_every steps (0: storage order)
+    int order_age = 0;                   // isf_step advections since the last sort
+    long long order_n = 0;               // slots of the current permutation (0: none)
+    const float* order_parts = nullptr;  // the slot array it was made for
+    isf::OrderBufs ord = {};
+    long long ord_cap = 0;               // slots the rank / order buffers hold
 };
 
 namespace isf_int {
@@ -91,6 +98,10 @@ int run_projection(isf_handle* h, float* psi, const JetArgs* jet);
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site);
 // the y / z transforms and the Laplacian multiply of the Poisson solve on h->F
 int run_poisson_spectral(isf_handle* h, const char* site);
+
+// the cell order of np slots on stream st (launch sites "<site> order count / scan / scatter")
+int ensure_order(isf_handle* h, long long np);
+int run_order(isf_handle* h, const float* parts, long long np, cudaStream_t st, const char* site);
 
 // releases the adjoint work buffers (isf_adj.cu)
 void adj_free(isf_handle* h);

@@ -105,8 +105,33 @@ cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, i
                               cudaStream_t s);
 // counters: 8 entries per simulation (clamp events, live particles, check records)
 constexpr int kCounterStride = 8;
+// order: null (storage order) or a permutation of the np slots to traverse them in
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel,
-                          unsigned long long* counters, cudaStream_t s, int nsim = 1, long long bs_vel = 0);
+                          unsigned long long* counters, cudaStream_t s, int nsim = 1, long long bs_vel = 0,
+                          const int* order = nullptr);
+
+// Cell order of the particle slots (k_particles.cu): a permutation of the np
+// slots, live ones grouped by 2 x 2 x 2 cell tile (tiles x fastest), dead
+// ones last.  Three steps on one stream: count (ranks within each key), scan
+// (the key counts to offsets), scatter (the permutation).
+struct OrderGeom {
+    float L[3], dinv[3];
+    int n[3], t[3];  // cells and tiles per axis
+    int nkeys;       // tiles + 1 (the dead slots' key)
+};
+struct OrderBufs {
+    unsigned* hist;   // order_keys(g) counts, then offsets
+    unsigned* rank;   // np: each slot's rank within its key
+    unsigned* sums;   // order_sums(g): per-tile sums of the scan
+    long long* total; // the scan's total (np)
+    int* order;       // np: the permutation
+};
+long long order_keys(const Grid& g);
+long long order_sums(const Grid& g);
+cudaError_t launch_order_count(const Grid& g, const float* parts, long long np, const OrderBufs& b, cudaStream_t s);
+cudaError_t launch_order_scan(const Grid& g, const OrderBufs& b, cudaStream_t s);
+cudaError_t launch_order_scatter(const Grid& g, const float* parts, long long np, const OrderBufs& b,
+                                 cudaStream_t s);
 
 // the Particles type of MatlabPort.jl: x, y, z vectors and active slot lists (k_particles.cu)
 cudaError_t launch_emit_soa(float* x, float* y, float* z, long long nslots, long long start, long long count,

@@ -34,10 +34,22 @@ __device__ __forceinline__ int cell_floor(float p, float dinv, float d, float ep
     return (fr > eps && fr < 1.f - eps) ? (int)f1 : __float2int_rd(__fdiv_rn(p, d));
 }
 
+// The same floor as a float (an integer value): the advection clamps it,
+// forms its weights and converts it once, with no int -> float round trip.
+template <bool POW2>
+__device__ __forceinline__ float cell_floor_f(float p, float dinv, float d, float eps) {
+    const float q1 = p * dinv;
+    const float f1 = floorf(q1);
+    if (POW2) return f1;
+    const float fr = q1 - f1;
+    return (fr > eps && fr < 1.f - eps) ? f1 : floorf(__fdiv_rn(p, d));
+}
+
 // The grid constants the advection needs, copied once into registers (the
 // kernel parameter is otherwise re-read at every RK stage).
 struct AdvConst {
     float L[3], d[3], dinv[3], feps[3];
+    float nmf[3];  // n - 1 as a float
     int nm[3];  // n - 1
     int pnx, pnxy;
     const float4* __restrict__ v;  // (vx, vy, vz, 0) per padded cell
@@ -53,6 +65,7 @@ __device__ __forceinline__ AdvConst adv_const(const Grid& g, const float* vel) {
         c.dinv[a] = g.dinv[a];
         c.feps[a] = g.feps[a];
         c.nm[a] = g.n[a] - 1;
+        c.nmf[a] = (float)(g.n[a] - 1);
     }
     c.pnx = g.pnx;
     c.pnxy = g.pnxy;

@@ -137,11 +137,13 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        int ii = cell_floor<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
-        clamps += (ii > k.nm[a]) ? 1u : 0u;  // mod rounded up to L
-        ii = max(min(ii, k.nm[a]), 0);
-        i[a] = ii;
-        w[a] = __fsub_rn(P[a], __fmul_rn((float)ii, k.d[a]));
+        // the cell floor, its clamp and the weight stay in float (integer
+        // values, exact); a NaN point clamps to cell 0 as an int floor would
+        float fl = cell_floor_f<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
+        clamps += (fl > k.nmf[a]) ? 1u : 0u;  // mod rounded up to L
+        fl = fminf(fmaxf(fl, 0.f), k.nmf[a]);
+        i[a] = __float2int_rz(fl);
+        w[a] = __fsub_rn(P[a], __fmul_rn(fl, k.d[a]));
         if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
     }
     (void)chk;
@@ -168,14 +170,19 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
 #undef ISF_IDX
 
 // staggered_advect! (parallel.jl:197-216, 248-261): classical RK4 for every
-// slot inside the open box 0 < p < L, (-1,-1,-1) otherwise.
+// slot inside the open box 0 < p < L, (-1,-1,-1) otherwise (a slot that holds
+// (-1,-1,-1) already is not stored again).
 // counters[0] accumulates clamp events, counters[1] live particles.
 // A batch launch advects simulation s = blockIdx.y: slots parts + s * 3 np,
 // velocity vel + s * bs_vel, counters + s * kCounterStride.
+// With `order` (a permutation of the np slots, cell-sorted by k_order_*),
+// thread t advects slot order[t]: the arithmetic of every slot is the same,
+// only the traversal changes.
 template <bool POW2, bool NORMW>
 __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
-                                                unsigned long long* __restrict__ counters, long long bs_vel) {
+                                                unsigned long long* __restrict__ counters, long long bs_vel,
+                                                const int* __restrict__ order) {
     pdl_enter();
     const int sim = blockIdx.y;
     parts += sim * 3LL * np;
@@ -184,7 +191,8 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
     unsigned clamps = 0, live = 0;
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
+        const int k = order ? __ldg(order + t) : t;
         float3 p = make_float3(parts[3 * k], parts[3 * k + 1], parts[3 * k + 2]);
         const bool inside = (p.x > 0.f && p.x < kc.L[0]) && (p.y > 0.f && p.y < kc.L[1]) &&
                             (p.z > 0.f && p.z < kc.L[2]);
@@ -202,6 +210,7 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
             p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
             p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
         } else {
+            if (p.x == -1.f && p.y == -1.f && p.z == -1.f) continue;  // dead already
             p = make_float3(-1.f, -1.f, -1.f);
         }
         parts[3 * k] = p.x;
@@ -429,6 +438,124 @@ __global__ void __launch_bounds__(256) k_gather3(const float* __restrict__ x, co
     block_add(&counters[12], bad);
 }
 
+// ---- cell order of the particle slots: the traversal of k_advect.
+// A slot's key is the 2 x 2 x 2 cell tile holding it (tiles x fastest), or
+// nkeys - 1 for a slot outside the open box (dead), so live particles come
+// out grouped by tile and the dead ones last.  Counting sort: k_order_count
+// takes each slot's rank within its key with an atomic (the order inside a
+// key is whatever the atomics give; every slot still appears exactly once),
+// an exclusive scan turns the key counts into offsets, k_order_scatter
+// places each slot.
+__device__ __forceinline__ int order_key(const OrderGeom& o, const float* __restrict__ parts, int s) {
+    const float x = parts[3 * s], y = parts[3 * s + 1], z = parts[3 * s + 2];
+    const bool inside = (x > 0.f && x < o.L[0]) && (y > 0.f && y < o.L[1]) && (z > 0.f && z < o.L[2]);
+    if (!inside) return o.nkeys - 1;
+    const int cx = min((int)(x * o.dinv[0]), o.n[0] - 1) >> 1;
+    const int cy = min((int)(y * o.dinv[1]), o.n[1] - 1) >> 1;
+    const int cz = min((int)(z * o.dinv[2]), o.n[2] - 1) >> 1;
+    return cx + o.t[0] * (cy + o.t[1] * cz);
+}
+
+__global__ void __launch_bounds__(256) k_order_count(OrderGeom o, const float* __restrict__ parts, int np,
+                                                     unsigned* __restrict__ hist, unsigned* __restrict__ rank) {
+    pdl_enter();
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < np; s += gridDim.x * blockDim.x)
+        rank[s] = atomicAdd(&hist[order_key(o, parts, s)], 1u);
+}
+
+__global__ void __launch_bounds__(256) k_order_scatter(OrderGeom o, const float* __restrict__ parts, int np,
+                                                       const unsigned* __restrict__ offs,
+                                                       const unsigned* __restrict__ rank, int* __restrict__ order) {
+    pdl_enter();
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < np; s += gridDim.x * blockDim.x)
+        order[offs[order_key(o, parts, s)] + rank[s]] = s;
+}
+
+// exclusive scan of n counts in place, in tiles of SCAN_ITEMS: per-tile sums,
+// a scan of the sums (k_keep_scan), then each tile's scan plus its offset
+constexpr int SCAN_T = 1024, SCAN_V = 4, SCAN_ITEMS = SCAN_T * SCAN_V;
+
+__device__ __forceinline__ unsigned block_exclusive(unsigned v) {
+    __shared__ unsigned wsum[SCAN_T / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const unsigned w = wsum[lane];
+        unsigned wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    return wsum[warp] + inc - v;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles(const unsigned* __restrict__ a, long long n,
+                                                       unsigned* __restrict__ sums) {
+    pdl_enter();
+    const long long base = (long long)blockIdx.x * SCAN_ITEMS + (long long)threadIdx.x * SCAN_V;
+    unsigned v = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_V; ++k)
+        if (base + k < n) v += a[base + k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __shared__ unsigned red[SCAN_T / 32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned t = red[threadIdx.x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) sums[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_apply(unsigned* __restrict__ a, long long n,
+                                                       const unsigned* __restrict__ offs) {
+    pdl_enter();
+    const long long base = (long long)blockIdx.x * SCAN_ITEMS + (long long)threadIdx.x * SCAN_V;
+    unsigned v[SCAN_V];
+    unsigned t = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_V; ++k) {
+        v[k] = base + k < n ? a[base + k] : 0u;
+        t += v[k];
+    }
+    unsigned run = offs[blockIdx.x] + block_exclusive(t);
+#pragma unroll
+    for (int k = 0; k < SCAN_V; ++k) {
+        if (base + k < n) a[base + k] = run;
+        run += v[k];
+    }
+}
+
+long long order_scan_tiles(long long nkeys) { return (nkeys + SCAN_ITEMS - 1) / SCAN_ITEMS; }
+
+OrderGeom order_geom(const Grid& g) {
+    OrderGeom o;
+    long long nk = 1;
+    for (int a = 0; a < 3; ++a) {
+        o.L[a] = g.L[a];
+        o.dinv[a] = g.dinv[a];
+        o.n[a] = g.n[a];
+        o.t[a] = (g.n[a] + 1) >> 1;
+        nk *= o.t[a];
+    }
+    o.nkeys = (int)(nk + 1);
+    return o;
+}
+
 namespace {
 unsigned grid_for(long long n, int blk) {
     long long b = (n + blk - 1) / blk;
@@ -521,7 +648,7 @@ cudaError_t launch_emit_batch(float* parts, long long nslots, long long count, i
 #endif
 
 cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float* vel, unsigned long long* counters,
-                          cudaStream_t s, int nsim, long long bs_vel) {
+                          cudaStream_t s, int nsim, long long bs_vel, const int* order) {
     if (np <= 0 || nsim <= 0) return cudaSuccess;
     if (np > kMaxParticles) return cudaErrorInvalidValue;
     const int blk = 256;
@@ -540,10 +667,46 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     const dim3 grid((unsigned)b, (unsigned)nsim);
     const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
     if (g.norm_w)
-        return pow2 ? launch_pdl(k_advect<true, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel)
-                    : launch_pdl(k_advect<false, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
-    return pow2 ? launch_pdl(k_advect<true, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel)
-                : launch_pdl(k_advect<false, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel);
+        return pow2 ? launch_pdl(k_advect<true, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
+                                 order)
+                    : launch_pdl(k_advect<false, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
+                                 order);
+    return pow2 ? launch_pdl(k_advect<true, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
+                             order)
+                : launch_pdl(k_advect<false, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
+                             order);
 }
+
+cudaError_t launch_order_count(const Grid& g, const float* parts, long long np, const OrderBufs& b, cudaStream_t s) {
+    if (np <= 0) return cudaSuccess;
+    if (np > kMaxParticles) return cudaErrorInvalidValue;
+    const OrderGeom o = order_geom(g);
+    cudaError_t e = cudaMemsetAsync(b.hist, 0, sizeof(unsigned) * (size_t)o.nkeys, s);
+    if (e != cudaSuccess) return e;
+    return launch_pdl(k_order_count, dim3(grid_for(np, 256)), dim3(256), 0, s, o, parts, (int)np, b.hist, b.rank);
+}
+
+cudaError_t launch_order_scan(const Grid& g, const OrderBufs& b, cudaStream_t s) {
+    const OrderGeom o = order_geom(g);
+    const long long ntiles = order_scan_tiles(o.nkeys);
+    cudaError_t e = launch_pdl(k_scan_tiles, dim3((unsigned)ntiles), dim3(SCAN_T), 0, s, (const unsigned*)b.hist,
+                               (long long)o.nkeys, b.sums);
+    if (e == cudaSuccess) e = launch_pdl(k_keep_scan, dim3(1), dim3(1024), 0, s, b.sums, ntiles, b.total);
+    if (e == cudaSuccess)
+        e = launch_pdl(k_scan_apply, dim3((unsigned)ntiles), dim3(SCAN_T), 0, s, b.hist, (long long)o.nkeys,
+                       (const unsigned*)b.sums);
+    return e;
+}
+
+cudaError_t launch_order_scatter(const Grid& g, const float* parts, long long np, const OrderBufs& b,
+                                 cudaStream_t s) {
+    if (np <= 0) return cudaSuccess;
+    const OrderGeom o = order_geom(g);
+    return launch_pdl(k_order_scatter, dim3(grid_for(np, 256)), dim3(256), 0, s, o, parts, (int)np,
+                      (const unsigned*)b.hist, (const unsigned*)b.rank, b.order);
+}
+
+long long order_keys(const Grid& g) { return order_geom(g).nkeys; }
+long long order_sums(const Grid& g) { return order_scan_tiles(order_geom(g).nkeys); }
 
 }  // namespace isf
