@@ -80,6 +80,40 @@ __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
+// The barrier of the threads that run one CTA's work: the whole CTA for a
+// kernel launched on its own (CtaBar), or the named barrier of one virtual
+// CTA, n threads of a larger block, in the persistent batch kernel
+// (NamedBar; ids 1..15, n a multiple of 32).
+struct CtaBar {
+    static constexpr bool kLaunch = true;
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct NamedBar {
+    static constexpr bool kLaunch = false;
+    int id, n;
+    __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+};
+
+// Block coordinates and thread index of one (virtual) CTA: blockIdx /
+// threadIdx for a kernel launched on its own, the work item's in the
+// persistent batch kernel.
+struct Blk {
+    int x, y, z, tid;
+};
+__device__ __forceinline__ Blk launch_blk() {
+    return Blk{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)threadIdx.x};
+}
+
+// A load of data that another pass writes: through the read-only path in a
+// kernel launched on its own (the data is constant for its lifetime), a
+// plain coherent load in the persistent batch kernel, where the writer ran
+// earlier in the same launch.
+template <class B, class T>
+__device__ __forceinline__ T ldm(const T* p) {
+    if constexpr (B::kLaunch) return __ldg(p);
+    else return *p;
+}
+
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float4 cadd(float4 a, float4 b) {

@@ -161,18 +161,19 @@ struct First {
 // Runs stages (P, R), Rest... on x, which holds the inputs of stage (P, R);
 // intermediate results go through the shared tile sm (pencil q), the final
 // outputs to dst.  Ends without a barrier after the final scatter.
-template <int N, int NT, int C, int S, class T, class Dst, int P, int R, int... Rest>
-__device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2* __restrict__ tw, const Dst& dst) {
+template <int N, int NT, int C, int S, class T, class Dst, class B, int P, int R, int... Rest>
+__device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2* __restrict__ tw, const Dst& dst,
+                                         const B& bar) {
     butterflies<N, NT, R, P, S>(x, t, tw);
     if constexpr (sizeof...(Rest) == 0) {
         scatter<N, NT, R, P>(x, t, dst);
     } else {
         scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
-        __syncthreads();
+        bar.sync();
         constexpr int R2 = First<Rest...>::value;
         gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
-        __syncthreads();
-        pipeline<N, NT, C, S, T, Dst, P * R, Rest...>(x, t, q, sm, tw, dst);
+        bar.sync();
+        pipeline<N, NT, C, S, T, Dst, B, P * R, Rest...>(x, t, q, sm, tw, dst, bar);
     }
 }
 
@@ -181,16 +182,16 @@ __device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2
 // exactly the input layout of a first stage of radix R with N / R
 // butterflies, so an inverse transform whose radices run in the reverse
 // order can start from these registers without a pass through shared memory.
-template <int N, int NT, int C, int S, class T, int P, int R, int... Rest>
-__device__ __forceinline__ void pipeline_keep(T* x, int t, int q, T* sm, const float2* __restrict__ tw) {
+template <int N, int NT, int C, int S, class T, class B, int P, int R, int... Rest>
+__device__ __forceinline__ void pipeline_keep(T* x, int t, int q, T* sm, const float2* __restrict__ tw, const B& bar) {
     butterflies<N, NT, R, P, S>(x, t, tw);
     if constexpr (sizeof...(Rest) > 0) {
         scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
-        __syncthreads();
+        bar.sync();
         constexpr int R2 = First<Rest...>::value;
         gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
-        __syncthreads();
-        pipeline_keep<N, NT, C, S, T, P * R, Rest...>(x, t, q, sm, tw);
+        bar.sync();
+        pipeline_keep<N, NT, C, S, T, B, P * R, Rest...>(x, t, q, sm, tw, bar);
     }
 }
 
@@ -219,21 +220,22 @@ struct Plan;
         static constexpr int NT = NN / R0;                                                                  \
         static constexpr int EMAX = isf_emax(NN, NN / R0, {ISF_UNPAREN FWD});                              \
         /* SYNC: barrier after the first gather (needed when src reads the tile) */                       \
-        template <int C, int S, bool SYNC, class T, class Src, class Dst>                                   \
+        template <int C, int S, bool SYNC, class T, class Src, class Dst, class B = CtaBar>                 \
         static __device__ __forceinline__ void run(T* x, int t, int q, T* sm, const float2* __restrict__ tw, \
-                                                   const Src& src, const Dst& dst) {                        \
+                                                   const Src& src, const Dst& dst, const B& bar = B()) {    \
             gather<NN, NN / R0, R0>(x, t, src);                                                             \
-            if constexpr (SYNC) __syncthreads();                                                            \
-            pipeline<NN, NN / R0, C, S, T, Dst, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, dst);                  \
+            if constexpr (SYNC) bar.sync();                                                                 \
+            pipeline<NN, NN / R0, C, S, T, Dst, B, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, dst, bar);          \
         }                                                                                                   \
         /* forward transform, mul(j, v) on every output j in registers, inverse transform */               \
-        template <int C, class T, class Src, class Mul, class Dst>                                          \
+        template <int C, class T, class Src, class Mul, class Dst, class B = CtaBar>                        \
         static __device__ __forceinline__ void run_spectral(T* x, int t, int q, T* sm,                      \
                                                             const float2* __restrict__ tw, const Src& src,  \
-                                                            const Mul& mul, const Dst& dst) {               \
+                                                            const Mul& mul, const Dst& dst,                 \
+                                                            const B& bar = B()) {                           \
             constexpr int NTh = NN / R0;                                                                    \
             gather<NN, NTh, R0>(x, t, src);                                                                 \
-            pipeline_keep<NN, NTh, C, -1, T, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw);                          \
+            pipeline_keep<NN, NTh, C, -1, T, B, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, bar);                  \
             constexpr int RL = First<ISF_UNPAREN REV>::value, PL = NN / RL;                                 \
             constexpr int NBT = Stage<NN, NTh, RL>::NBT;                                                    \
             _Pragma("unroll") for (int b = 0; b < NBT; ++b) {                                               \
@@ -242,7 +244,7 @@ struct Plan;
                     _Pragma("unroll") for (int r = 0; r < RL; ++r) x[b * RL + r] = mul(i + r * PL, x[b * RL + r]); \
                 }                                                                                           \
             }                                                                                               \
-            pipeline<NN, NTh, C, +1, T, Dst, 1, ISF_UNPAREN REV>(x, t, q, sm, tw, dst);                     \
+            pipeline<NN, NTh, C, +1, T, Dst, B, 1, ISF_UNPAREN REV>(x, t, q, sm, tw, dst, bar);             \
         }                                                                                                   \
     };
 

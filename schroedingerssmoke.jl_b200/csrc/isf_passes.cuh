@@ -69,21 +69,20 @@ struct XShape {
     static constexpr size_t SMEM = (size_t)G * N * C * sizeof(typename XTraits<OP>::T);
 };
 
-template <int N, int OP, int G>
-__global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
-    pdl_enter();
+template <int N, int OP, int G, class BarT = CtaBar>
+__device__ __forceinline__ void xpass_body(const XArgs& a, const Blk& bk, unsigned char* smraw,
+                                           const BarT& bar = BarT()) {
     using Tr = XTraits<OP>;
     using T = typename Tr::T;
     constexpr int C = Tr::C;
     constexpr int NT = Plan<N>::NT;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    const int grp = bk.tid / (C * NT), lt = bk.tid % (C * NT);
     T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
     const int t = lt % NT, q = lt / NT;
-    const long long row = ((long long)blockIdx.x * G + grp) * C + q;
+    const long long row = ((long long)bk.x * G + grp) * C + q;
     const long long rb = row * N;
-    float4* __restrict__ psi = a.psi + blockIdx.y * a.bs_psi;
-    float2* __restrict__ F = a.F + blockIdx.y * a.bs_F;
+    float4* __restrict__ psi = a.psi + bk.y * a.bs_psi;
+    float2* __restrict__ F = a.F + bk.y * a.bs_F;
     T x[Plan<N>::EMAX];
 
     auto src = [&](int j) -> T {
@@ -103,7 +102,14 @@ __global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
             F[rb + j] = v;
         }
     };
-    Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst);
+    Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst, bar);
+}
+
+template <int N, int OP, int G>
+__global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    xpass_body<N, OP, G>(a, launch_blk(), smraw);
 }
 
 // ------------------------------------------- x pass of real data (Poisson)
@@ -134,30 +140,29 @@ struct XRShape {
     static constexpr size_t SMEM = (size_t)G * (KM && STAGE > TILE ? STAGE : TILE);
 };
 
-template <int N, int OP, int G, bool KM = false>
-__global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
-    pdl_enter();
+template <int N, int OP, int G, bool KM = false, class BarT = CtaBar>
+__device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsigned char* smraw,
+                                           const BarT& bar = BarT()) {
     using T = float2;
     constexpr int C = 16;
     constexpr int NT = Plan<N>::NT;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    const int grp = bk.tid / (C * NT), lt = bk.tid % (C * NT);
     T* sm = reinterpret_cast<T*>(smraw + grp * XRShape<N, G, KM>::SMEM / G);
     const int t = lt % NT, q = lt / NT;
-    const long long rbase = 2 * ((long long)blockIdx.x * G + grp) * C;  // first row of the group
+    const long long rbase = 2 * ((long long)bk.x * G + grp) * C;  // first row of the group
     const long long r0 = rbase + 2 * q;
     const int wp = a.wp;
     const int ny = a.g.n[1], nz = a.g.n[2];
-    const int sim = blockIdx.y;
+    const int sim = bk.y;
     float2* __restrict__ Fs = a.F + sim * a.bs_F;
     T x[Plan<N>::EMAX];
     if constexpr (OP == XR_FWD) {
         const float* __restrict__ f0 = a.rin + sim * a.bs_r + r0 * N;
         const float* __restrict__ f1 = f0 + N;
-        auto src = [&](int j) -> T { return make_float2(__ldg(&f0[j]), __ldg(&f1[j])); };
+        auto src = [&](int j) -> T { return make_float2(ldm<BarT>(&f0[j]), ldm<BarT>(&f1[j])); };
         auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
-        Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst);
-        __syncthreads();
+        Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst, bar);
+        bar.sync();
         if constexpr (KM) {
             // lanes over the row pairs of the group: 16 x 16 B per k
             float4* __restrict__ F4 = reinterpret_cast<float4*>(Fs);
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
                 const int y = (int)(r % ny), z = (int)(r / ny);
                 stg[k * C + (qq ^ (k & (C - 1)))] = F4[(((long long)k * nz + z) * ny + y) >> 1];
             }
-            __syncthreads();
+            bar.sync();
         }
         float* __restrict__ rout = a.rout + sim * a.bs_r;
         float4* __restrict__ psi = a.psi + sim * a.bs_psi;
@@ -234,8 +239,15 @@ __global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
         };
         // k-major: the staging aliases the tile, so the first gather must
         // complete before the first stage writes the tile
-        Plan<N>::template run<C, +1, KM>(x, t, q, sm, a.g.tw[0], src, dst);
+        Plan<N>::template run<C, +1, KM>(x, t, q, sm, a.g.tw[0], src, dst, bar);
     }
+}
+
+template <int N, int OP, int G, bool KM = false>
+__global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    xreal_body<N, OP, G, KM>(a, launch_blk(), smraw);
 }
 
 // ------------------------------------------- Poisson solve on (y, z) planes
@@ -257,12 +269,12 @@ struct PlaneArgs {
 #define ISF_PLANE_MAX_THREADS 1024
 #endif
 
-template <int N>
+template <int N, int MAXT = ISF_PLANE_MAX_THREADS>
 struct PlaneShape {
     static constexpr int C = 16;
     static constexpr int NT = Plan<N>::NT;
     static constexpr int GT = C * NT;  // threads of one pencil group
-    static constexpr int GMAX = ISF_PLANE_MAX_THREADS / GT > 0 ? ISF_PLANE_MAX_THREADS / GT : 1;
+    static constexpr int GMAX = MAXT / GT > 0 ? MAXT / GT : 1;
     static constexpr int GROUPS = GMAX < (N / C) ? GMAX : (N / C);
     static constexpr int BLK = GROUPS * GT;
     static constexpr int ROUNDS = (N / C + GROUPS - 1) / GROUPS;
@@ -270,17 +282,15 @@ struct PlaneShape {
     static_assert(N % C == 0, "plane width");
 };
 
-template <int N>
-__global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs a) {
-    pdl_enter();
-    using Sh = PlaneShape<N>;
+template <int N, class Sh = PlaneShape<N>, class BarT = CtaBar>
+__device__ __forceinline__ void plane_body(const PlaneArgs& a, const Blk& bk, unsigned char* smraw,
+                                           const BarT& bar = BarT()) {
     constexpr int C = Sh::C, NT = Sh::NT, GT = Sh::GT;
-    extern __shared__ __align__(16) unsigned char smraw[];
     float2* plane = reinterpret_cast<float2*>(smraw);
-    const int grp = threadIdx.x / GT, lt = threadIdx.x % GT;
+    const int grp = bk.tid / GT, lt = bk.tid % GT;
     float2* tile = plane + N * N + grp * (N * C);
-    const int kx = blockIdx.x;
-    float2* __restrict__ Fp = a.F + blockIdx.y * a.bs_F + (long long)kx * N * N;
+    const int kx = bk.x;
+    float2* __restrict__ Fp = a.F + bk.y * a.bs_F + (long long)kx * N * N;
     float2 x[Plan<N>::EMAX];
     const float2 zero = make_float2(0.f, 0.f);
     // y transforms: pencil = row z of the plane, lanes along y.  The forward
@@ -304,8 +314,8 @@ __global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs 
                 else
                     Fp[z * N + j] = v;
             };
-            Plan<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst);
-            __syncthreads();
+            Plan<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst, bar);
+            bar.sync();
         }
     };
     ysweep(std::integral_constant<int, -1>());
@@ -332,11 +342,18 @@ __global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs 
                 const float f = (zero_line && j == 0) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2z[j])));
                 return cscale(v, f);
             };
-            Plan<N>::template run_spectral<C>(x, t, q, tile, a.g.tw[2], src, fmul, dst);
-            __syncthreads();
+            Plan<N>::template run_spectral<C>(x, t, q, tile, a.g.tw[2], src, fmul, dst, bar);
+            bar.sync();
         }
     }
     ysweep(std::integral_constant<int, +1>());
+}
+
+template <int N>
+__global__ void __launch_bounds__(PlaneShape<N>::BLK) k_poisson_plane(PlaneArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    plane_body<N>(a, launch_blk(), smraw);
 }
 
 // -------------------------------------------------------------- y / z pass
@@ -388,18 +405,17 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-template <int N, class T, int OP, int G>
-__global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G>::MINB) k_yzpass(YZArgs a) {
-    pdl_enter();
+template <int N, class T, int OP, int G, class BarT = CtaBar>
+__device__ __forceinline__ void yzpass_body(const YZArgs& a, const Blk& bk, unsigned char* smraw,
+                                            const BarT& bar = BarT()) {
     constexpr int C = YZShape<N, T>::C;
     constexpr int NT = Plan<N>::NT;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int grp = threadIdx.x / (C * NT), lt = threadIdx.x % (C * NT);
+    const int grp = bk.tid / (C * NT), lt = bk.tid % (C * NT);
     T* sm = reinterpret_cast<T*>(smraw) + grp * (N * C);
     const int q = lt % C, t = lt / C;
     const int rl = a.row, ny = a.g.n[1];
-    const int x0 = blockIdx.x * C;
-    const int o = blockIdx.y * G + grp;
+    const int x0 = bk.x * C;
+    const int o = bk.y * G + grp;
     long long stride, base;
     if (a.axis == 1) {
         stride = rl;
@@ -408,7 +424,7 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
         stride = (long long)rl * ny;
         base = x0 + (long long)o * rl;
     }
-    T* __restrict__ data = reinterpret_cast<T*>(a.data) + blockIdx.z * a.bstride;
+    T* __restrict__ data = reinterpret_cast<T*>(a.data) + bk.z * a.bstride;
     const float2* tw = a.g.tw[a.axis];
     T x[Plan<N>::EMAX];
 
@@ -416,9 +432,9 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
     auto gdst = [&](int j, const T& v) { data[base + j * stride + q] = v; };
 
     if constexpr (OP == YZ_FWD) {
-        Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, gdst);
+        Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, gdst, bar);
     } else if constexpr (OP == YZ_INV) {
-        Plan<N>::template run<C, +1, false>(x, t, q, sm, tw, gsrc, gdst);
+        Plan<N>::template run<C, +1, false>(x, t, q, sm, tw, gsrc, gdst, bar);
     } else {
         // spectral multiply between the forward and the inverse transform of
         // this pencil; k along the pass axis is the pencil position j
@@ -438,7 +454,7 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
                 m.y *= msign;
                 return cmul(v, make_float2((float)m.x, (float)m.y));
             };
-            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, mmul, gdst);
+            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, mmul, gdst, bar);
         } else {
             static_assert(OP == YZ_FAC, "unhandled y/z op");
             // fac(k)/N, fac = -0.25 / sum_a (sin(pi k_a / n_a) / d_a)^2, fac(0) = 0
@@ -452,9 +468,16 @@ __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G
                 const float f = (pad || (zero_line && j == 0)) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2[j])));
                 return cscale(v, f);
             };
-            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, fmul, gdst);
+            Plan<N>::template run_spectral<C>(x, t, q, sm, tw, gsrc, fmul, gdst, bar);
         }
     }
+}
+
+template <int N, class T, int OP, int G>
+__global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G>::MINB) k_yzpass(YZArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    yzpass_body<N, T, OP, G>(a, launch_blk(), smraw);
 }
 
 }  // namespace isf

@@ -5,69 +5,6 @@
 
 namespace isf {
 
-// Philox4x32-10 (Salmon et al., SC'11): ten rounds of two 32x32->64-bit
-// multiplies, round keys bumped by the Weyl constants after each round.
-struct U4 {
-    uint32_t v[4];
-};
-__device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
-    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
-    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        const uint32_t hi0 = __umulhi(M0, c.v[0]), lo0 = M0 * c.v[0];
-        const uint32_t hi1 = __umulhi(M1, c.v[2]), lo1 = M1 * c.v[2];
-        U4 n;
-        n.v[0] = hi1 ^ c.v[1] ^ k0;
-        n.v[1] = lo1;
-        n.v[2] = hi0 ^ c.v[3] ^ k1;
-        n.v[3] = lo0;
-        c = n;
-        k0 += W0;
-        k1 += W1;
-    }
-    return c;
-}
-__device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
-
-// add_particles! (particles.jl:30-94) with a seeded counter-based stream.
-// Stream: counter = (j, counter_lo, counter_hi, 0x15F0015F), key = seed.
-// mode 0: the reference ring (0.9 r around (x - 0.1) with +-0.05 jitter,
-//         particles.jl:86-90); 1: uniform in the nozzle disc at x = cen.x;
-//         2: uniform in the nozzle cylinder; 3: the MatlabPort driver's ring
-//         (0.9 r in the plane x = cen.x, no jitter,
-//         examples/matlabport/simple.jl:112-115).
-__device__ __forceinline__ float3 emit_point(long long j, const EmitArgs& e) {
-    U4 c = {{(uint32_t)j, (uint32_t)e.counter, (uint32_t)(e.counter >> 32), 0x15F0015Fu}};
-    const U4 r = philox4x32_10(c, (uint32_t)e.seed, (uint32_t)(e.seed >> 32));
-    const float u0 = u01(r.v[0]), u1 = u01(r.v[1]), u2 = u01(r.v[2]), u3 = u01(r.v[3]);
-    const float pi = 3.14159265358979323846f;
-    float p0, p1, p2;
-    if (e.mode == 0 || e.mode == 3) {
-        const float rt = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
-        const float rr = __fmul_rn(0.9f, e.rad);
-        if (e.mode == 3) {
-            p0 = e.cen[0];
-            p1 = __fadd_rn(e.cen[1], __fmul_rn(rr, cosf(rt)));
-            p2 = __fadd_rn(e.cen[2], __fmul_rn(rr, sinf(rt)));
-        } else {
-            const float o0 = __fsub_rn(__fmul_rn(u1, 0.1f), 0.05f);
-            const float o1 = __fsub_rn(__fmul_rn(u2, 0.1f), 0.05f);
-            const float o2 = __fsub_rn(__fmul_rn(u3, 0.1f), 0.05f);
-            p0 = __fadd_rn(__fsub_rn(e.cen[0], 0.1f), o0);
-            p1 = __fadd_rn(__fadd_rn(e.cen[1], __fmul_rn(rr, cosf(rt))), o1);
-            p2 = __fadd_rn(__fadd_rn(e.cen[2], __fmul_rn(rr, sinf(rt))), o2);
-        }
-    } else {
-        const float th = __fmul_rn(__fmul_rn(u0, 2.0f), pi);
-        const float rho = __fmul_rn(e.rad, sqrtf(u1));
-        p0 = (e.mode == 1) ? e.cen[0] : __fadd_rn(e.cen[0], __fmul_rn(__fsub_rn(u2, 0.5f), e.len));
-        p1 = __fadd_rn(e.cen[1], __fmul_rn(rho, cosf(th)));
-        p2 = __fadd_rn(e.cen[2], __fmul_rn(rho, sinf(th)));
-    }
-    return make_float3(p0, p1, p2);
-}
-
 // Particles of slot array(s) parts; a batch launch (emits != null) handles
 // simulation s = blockIdx.y with emits[s] and its own slots parts + s * 3 * nslots.
 __global__ void k_emit(float* __restrict__ parts, long long nslots, long long start, long long count, EmitArgs e,
@@ -101,74 +38,6 @@ __global__ void k_emit_soa(float* __restrict__ x, float* __restrict__ y, float* 
     z[s] = p.z;
 }
 
-#ifdef ISF_CHECK
-// debug builds: validate a gather index, record the first bad one, read cell 0
-__device__ __forceinline__ int checked(const AdvConst& k, int c, unsigned long long* chk, const int i[3]) {
-    if (c < 0 || (long long)c >= k.NP) {
-        if (chk && atomicAdd(&chk[0], 1ull) == 0) {
-            chk[1] = (unsigned long long)(unsigned)c;
-            for (int a = 0; a < 3; ++a) chk[2 + a] = (unsigned long long)(unsigned)i[a];
-        }
-        return 0;
-    }
-    return c;
-}
-#define ISF_IDX(c) checked(k, (c), chk, i)
-#else
-#define ISF_IDX(c) (c)
-#endif
-
-// staggered_velocity (parallel.jl:219-246) on the handle's padded velocity
-// grid: seven 16-byte gathers (the cells whose components the reference's
-// twelve samples need).  Interpolation weights are the reference's unnormalised
-// w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
-// clamped to the last cell and counted.
-template <bool POW2, bool NORMW>
-__device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigned& clamps, unsigned long long* chk) {
-    float P[3] = {pt.x, pt.y, pt.z};
-    // mod.(point, ph_size): identity for points inside the box (the common case)
-    const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
-                       (pt.z >= 0.f && pt.z < k.L[2]);
-    if (!inbox) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], k.L[a]);
-    }
-    int i[3];
-    float w[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        // the cell floor, its clamp and the weight stay in float (integer
-        // values, exact); a NaN point clamps to cell 0 as an int floor would
-        float fl = cell_floor_f<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
-        clamps += (fl > k.nmf[a]) ? 1u : 0u;  // mod rounded up to L
-        fl = fminf(fmaxf(fl, 0.f), k.nmf[a]);
-        i[a] = __float2int_rz(fl);
-        w[a] = __fsub_rn(P[a], __fmul_rn(fl, k.d[a]));
-        if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
-    }
-    (void)chk;
-    // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell
-    const int sy = k.pnx, sz = k.pnxy;
-    const int c000 = i[0] + sy * i[1] + sz * i[2];
-    const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
-    // the reference's 12 samples (parallel.jl:224-234) from 7 cells
-    const float4 a000 = __ldg(k.v + ISF_IDX(c000)), a100 = __ldg(k.v + ISF_IDX(c100));
-    const float4 a010 = __ldg(k.v + ISF_IDX(c010)), a001 = __ldg(k.v + ISF_IDX(c001));
-    const float4 a011 = __ldg(k.v + ISF_IDX(c010 + sz)), a101 = __ldg(k.v + ISF_IDX(c100 + sz));
-    const float4 a110 = __ldg(k.v + ISF_IDX(c100 + sy));
-    const float x00 = a000.x, x10 = a010.x, x01 = a001.x, x11 = a011.x;
-    const float y00 = a000.y, y10 = a100.y, y01 = a001.y, y11 = a101.y;
-    const float z00 = a000.z, z10 = a100.z, z01 = a010.z, z11 = a110.z;
-    const float wx = w[0], wy = w[1], wz = w[2];
-    float3 u;
-    // u_x bilinear in (y, z), u_y in (x, z), u_z in (x, y) (parallel.jl:230-245)
-    u.x = (1.f - wz) * ((1.f - wy) * x00 + wy * x10) + wz * ((1.f - wy) * x01 + wy * x11);
-    u.y = (1.f - wz) * ((1.f - wx) * y00 + wx * y10) + wz * ((1.f - wx) * y01 + wx * y11);
-    u.z = (1.f - wy) * ((1.f - wx) * z00 + wx * z10) + wy * ((1.f - wx) * z01 + wx * z11);
-    return u;
-}
-#undef ISF_IDX
-
 // staggered_advect! (parallel.jl:197-216, 248-261): classical RK4 for every
 // slot inside the open box 0 < p < L, (-1,-1,-1) otherwise (a slot that holds
 // (-1,-1,-1) already is not stored again).
@@ -191,32 +60,8 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
     unsigned clamps = 0, live = 0;
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x) {
-        const int k = order ? __ldg(order + t) : t;
-        float3 p = make_float3(parts[3 * k], parts[3 * k + 1], parts[3 * k + 2]);
-        const bool inside = (p.x > 0.f && p.x < kc.L[0]) && (p.y > 0.f && p.y < kc.L[1]) &&
-                            (p.z > 0.f && p.z < kc.L[2]);
-        if (inside) {
-            ++live;
-            // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
-            const float3 k1 = stag_vel<POW2, NORMW>(kc, p, clamps, chk);
-            float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-            const float3 k2 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
-            q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-            const float3 k3 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
-            q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-            const float3 k4 = stag_vel<POW2, NORMW>(kc, q, clamps, chk);
-            p.x = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
-            p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
-            p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);
-        } else {
-            if (p.x == -1.f && p.y == -1.f && p.z == -1.f) continue;  // dead already
-            p = make_float3(-1.f, -1.f, -1.f);
-        }
-        parts[3 * k] = p.x;
-        parts[3 * k + 1] = p.y;
-        parts[3 * k + 2] = p.z;
-    }
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x)
+        advect_slot<POW2, NORMW>(kc, parts, order ? __ldg(order + t) : t, dt, s6, clamps, live, chk);
     if (counters) {
         // block-aggregated counters: one atomic per CTA and counter
         __shared__ unsigned red[2][8];
