@@ -308,6 +308,25 @@ def batched_vs_plain(pkg, cfgs, steps, warmup, local):
     t_batch = e0.elapsed_time(e1)
     ncls, _ = b.classes()
     tiles = {str(c): b.tiles(c) for c in range(ncls)}
+    # the same ensemble as one persistent launch per call (all `steps` steps
+    # as work items of one kernel, bounded device-side waits between passes)
+    persistent = None
+    try:
+        b.set_persistent(True)
+        b.step(warmup)
+        b.sync()
+        e0.record(b.stream)
+        b.step(steps)
+        e1.record(b.stream)
+        e1.synchronize()
+        b.sync()
+        t_pers = e0.elapsed_time(e1)
+        persistent = {"value": len(sims) * steps / (t_pers / 1000.0), "unit": "sim-steps/s",
+                      "ms_per_ensemble_step": t_pers / steps, "launches_per_call": 1,
+                      "what": "isf_batch_set_persistent: one graph-captured launch of the persistent kernel per "
+                              "isf_batch_step call"}
+    except pkg.ISFError as err:
+        persistent = {"unavailable": str(err)}
     b.close()
 
     # the same simulations, one plain run after another
@@ -351,7 +370,9 @@ def batched_vs_plain(pkg, cfgs, steps, warmup, local):
             "grids": {str(g): sum(1 for s in sims if tuple(s["dims"]) == g[0]) for g in cfgs.ENSEMBLE_GRIDS},
             "value": n * steps / (t_batch / 1000.0), "unit": "sim-steps/s",
             "sequential_value": n * steps / (t_seq / 1000.0), "ratio_vs_sequential": t_seq / t_batch,
-            "ms_per_ensemble_step": t_batch / steps, "classes": ncls, "tiles": tiles}
+            "ms_per_ensemble_step": t_batch / steps, "classes": ncls, "tiles": tiles,
+            "persistent": (dict(persistent, ratio_vs_sequential=t_seq / (n * steps / persistent["value"] * 1000.0))
+                           if persistent and "value" in persistent else persistent)}
 
 
 def sharded_ensemble(pkg, cfgs, steps, warmup, rank, world, local):

@@ -44,6 +44,7 @@ enum {
     ISF_ERR_CUDA = 2,        /* CUDA runtime error (message has the CUDA text) */
     ISF_ERR_NOMEM = 3,       /* device allocation failed */
     ISF_ERR_NAN = 4,         /* isf_step with ISF_FLAG_CHECK_NAN found a non-finite psi */
+    ISF_ERR_TIMEOUT = 5,     /* a bounded device-side wait of the persistent batch kernel ran out */
 };
 
 /* isf_params.flags */
@@ -358,6 +359,25 @@ ISF_API int isf_batch_step(isf_batch* b, int32_t nsteps);
 ISF_API int isf_batch_set_step(isf_batch* b, int64_t step);
 ISF_API int isf_batch_get_stream(const isf_batch* b, void** stream);
 ISF_API int isf_batch_sync(isf_batch* b);
+
+/* The persistent batch kernel.  With mode ISF_PERSIST_ON, isf_batch_step(b,
+ * k) runs all k ensemble steps as one launch of one persistent kernel
+ * (captured in a CUDA graph per k, after a zeroing of its work counters).
+ * Its blocks take work items in order from one counter: an item is a few
+ * CTAs' worth of one pass of one class (the passes of isf_step, the same
+ * arithmetic, so results are bitwise those of the per-step graph and of
+ * isf_step).  A pass waits on the device for the pass before it in its
+ * class's chain with a bounded poll: after spin_limit polls (<= 0: the
+ * default, 2^22, about a second) the kernel records ISF_ERR_TIMEOUT, every
+ * block stops at its next item, and isf_batch_sync returns ISF_ERR_TIMEOUT
+ * naming the pass; the state is then partly stepped.  ISF_PERSIST_STALL adds
+ * a wait on a flag that nothing sets to every dependent pass, so the timeout
+ * path can be exercised without a fault.  Needs every class to have nx in
+ * {16,32,48,64,96,128} and ny = nz in {32,48,64,96} (ISF_ERR_INVALID
+ * otherwise).  Mode 0 returns to the per-step graph.  Reference: the
+ * ensemble is new; each simulation's step is examples/benchmark.jl:46-65. */
+enum { ISF_PERSIST_ON = 1, ISF_PERSIST_STALL = 2 };
+ISF_API int isf_batch_set_persistent(isf_batch* b, int32_t mode, int64_t spin_limit);
 /* number of classes, and the class of every simulation (nsims entries, may be NULL) */
 ISF_API int isf_batch_info(const isf_batch* b, int32_t* nclasses, int32_t* sim_class);
 /* the autotuned tile of each pass kind (ISF_TILE_*) of class cls */

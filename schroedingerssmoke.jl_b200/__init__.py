@@ -445,6 +445,15 @@ class ISFBatch:
     def set_step(self, k: int):
         self._chk(self.L.isf_batch_set_step(self.b, int(k)))
 
+    def set_persistent(self, on: bool = True, spin_limit: int = 0, stall: bool = False):
+        """Run each step(k) call as one launch of the persistent batch kernel
+        (isf_batch_set_persistent); spin_limit bounds each device-side wait
+        (<= 0: the default); stall makes the dependent passes wait on a flag
+        nothing sets, so the launch times out (sync raises ISFError with
+        ISF_ERR_TIMEOUT)."""
+        mode = (_lib.PERSIST_ON if on else 0) | (_lib.PERSIST_STALL if stall else 0)
+        self._chk(self.L.isf_batch_set_persistent(self.b, mode, int(spin_limit)))
+
     def sync(self):
         self._chk(self.L.isf_batch_sync(self.b))
 

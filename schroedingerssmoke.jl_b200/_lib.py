@@ -11,7 +11,8 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libisf.so")
 
-ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM, ISF_ERR_NAN = 0, 1, 2, 3, 4
+ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM, ISF_ERR_NAN, ISF_ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
+PERSIST_ON, PERSIST_STALL = 1, 2
 FLAG_NORMALIZED_WEIGHTS, FLAG_CHECK_NAN = 1, 2
 PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
 EMIT_RING, EMIT_DISC, EMIT_CYLINDER, EMIT_RING_PLANE = 0, 1, 2, 3
@@ -34,7 +35,7 @@ EXPORTS = (
     "isf_psi_from_f64", "isf_psi_to_f64", "isf_velocity_from_f64", "isf_velocity_to_f64", "isf_real_from_f64",
     "isf_real_to_f64", "isf_complex_to_f64", "isf_gauge_transform", "isf_add_particles_soa",
     "isf_staggered_velocity", "isf_advect_active", "isf_keep_inside", "isf_gather_particles",
-    "isf_set_particle_order", "isf_sort_particles", "isf_get_particle_order",
+    "isf_set_particle_order", "isf_sort_particles", "isf_get_particle_order", "isf_batch_set_persistent",
 )
 TILE_KINDS = ("x_psi", "x_real", "y_psi", "z_psi", "y_half", "z_half")
 
@@ -152,6 +153,7 @@ def load(path: str | None = None):
         "isf_staggered_advect": [vp, vp, i64],
         "isf_step": [vp, vp, vp, i64, C.POINTER(IsfStepArgs)],
         "isf_set_particle_order": [vp, i32],
+        "isf_batch_set_persistent": [vp, i32, i64],
         "isf_sort_particles": [vp, vp, i64],
         "isf_get_particle_order": [vp, vp, i64, C.POINTER(i64)],
         "isf_div": [vp, vp],

@@ -25,15 +25,10 @@
 #include "../../include/isf.h"
 #include "isf_launch.h"
 #include "isf_passes.cuh"
+#include "isf_persist.h"
 
 namespace isf {
 namespace {
-
-// per-simulation run-time constants of the prologue
-struct SimRT {
-    float omega, dt;
-    long long count, nslots;
-};
 
 // Step counter and per-simulation jet / emission arguments of step it =
 // counter + 1: omega t with t = Float32(it) * dt (every product rounded as
@@ -106,6 +101,23 @@ struct isf_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::string err;
+    // the persistent kernel (isf_batch_set_persistent): its phase table, one
+    // CUDA graph per step count (zero the counters, one launch), the status
+    int mode = 0;                  // ISF_PERSIST_* bits; 0: the per-step graph
+    bool persist_ok = false;       // every class fits the persistent kernel
+    std::string persist_why;
+    std::vector<PPhase> phases;    // slot order
+    std::vector<int> slot_start;   // items_per_step prefix
+    PPhase* d_ph = nullptr;
+    int* d_slot = nullptr;
+    unsigned* d_done = nullptr;
+    long long done_cap = 0;        // steps the done counters hold
+    unsigned* d_ctl = nullptr;
+    int* d_status = nullptr;
+    long long spin_limit = 1LL << 22;
+    int pgrid = 0, psmem = 0;
+    int pvper_div = 1;             // tuned: virtual CTAs per item = max / pvper_div
+    std::map<int, cudaGraphExec_t> pgraphs;
 };
 
 namespace {
@@ -327,7 +339,10 @@ int tune_class(isf_batch* b, BatchClass& c) {
     return rc;
 }
 
+void free_persist(isf_batch* b);
+
 void free_batch(isf_batch* b) {
+    free_persist(b);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (BatchClass& c : b->cls) {
@@ -380,6 +395,276 @@ int capture_step(isf_batch* b) {
     }
     b->graph = graph;
     return ISF_OK;
+}
+
+// ---- the persistent kernel: phase table, tuning, launch
+
+void free_persist(isf_batch* b) {
+    for (auto& kv : b->pgraphs) cudaGraphExecDestroy(kv.second);
+    b->pgraphs.clear();
+    cudaFree(b->d_ph);
+    cudaFree(b->d_slot);
+    cudaFree(b->d_done);
+    cudaFree(b->d_ctl);
+    cudaFree(b->d_status);
+    b->d_ph = nullptr;
+    b->d_slot = nullptr;
+    b->d_done = nullptr;
+    b->d_ctl = nullptr;
+    b->d_status = nullptr;
+    b->done_cap = 0;
+}
+
+PPhase new_phase(const BatchClass& c, int ci, int kind, int len, int gx, int gy, int gz) {
+    PPhase p;
+    std::memset(&p, 0, sizeof(p));
+    p.kind = kind;
+    p.cls = ci;
+    p.len = len;
+    p.gx = gx;
+    p.gy = gy;
+    p.tiles = gx * gy * gz;
+    p.dep = p.dep_prev = -1;
+    p.g = c.g;
+    p.first = c.first;
+    p.nsim = c.nsim;
+    return p;
+}
+
+// the pass chain of class_step for class ci, one phase per launch of it
+bool class_chain(const isf_batch* b, const BatchClass& c, int ci, std::vector<PPhase>& out, std::string& why) {
+    const int nx = c.g.n[0], ny = c.g.n[1], nz = c.g.n[2], ns = c.nsim;
+    if (!c.kmajor || !persist_plane_ok(ny) || !persist_len_ok(nx)) {
+        why = "class " + std::to_string(ci) + " (" + std::to_string(nx) + "x" + std::to_string(ny) + "x" +
+              std::to_string(nz) + "): the persistent kernel needs nx in {16,32,48,64,96,128} and ny = nz in "
+              "{32,48,64,96}";
+        return false;
+    }
+    const int rows = ny * nz;
+    auto up = [](long long a, long long d) { return (int)((a + d - 1) / d); };
+    out.push_back(new_phase(c, ci, PK_PROLOGUE, 0, 1, 1, 1));
+    auto xphase = [&](int kind) {
+        PPhase p = new_phase(c, ci, kind, nx, rows / 8, ns, 1);
+        p.x = bx(c, 1);
+        out.push_back(p);
+    };
+    auto yzphase = [&](int kind, int axis) {
+        PPhase p = new_phase(c, ci, kind, axis == 1 ? ny : nz, nx / 8, axis == 1 ? nz : ny, ns);
+        p.yz = byz(c, false, axis, 1);
+        out.push_back(p);
+    };
+    xphase(PK_X_FWD);
+    yzphase(PK_Y_FWD, 1);
+    yzphase(PK_Z_MASK, 2);
+    yzphase(PK_Y_INV, 1);
+    xphase(PK_X_INV_NORM);
+    auto projection = [&](const JetArgs* jets) {
+        PPhase d = new_phase(c, ci, PK_DIV, 0, up(nx, 32), up(ny, 16), up(nz, 8) * ns);
+        d.st = bst(c, c.f, c.g.N);
+        PPhase f = new_phase(c, ci, PK_XR_FWD, nx, rows / 32, ns, 1);
+        f.x = bx(c, 1);
+        PPhase pl = new_phase(c, ci, PK_PLANE, ny, nx / 2 + 1, ns, 1);
+        pl.pl.g = c.g;
+        pl.pl.F = c.F;
+        pl.pl.bs_F = c.bs_F();
+        PPhase gi = new_phase(c, ci, PK_XR_INV_GAUGE, nx, rows / 32, ns, 1);
+        gi.x = bx(c, 1);
+        if (jets) {
+            d.st.use_jet = 1;
+            d.st.jets = jets;
+            gi.x.use_jet = 1;
+            gi.x.jets = jets;
+        }
+        out.push_back(d);
+        out.push_back(f);
+        out.push_back(pl);
+        out.push_back(gi);
+    };
+    projection(nullptr);
+    if (c.key.jet) {
+        if (c.key.emit > 0 && c.key.nslots > 0) {
+            PPhase e = new_phase(c, ci, PK_EMIT, 0, up(c.key.emit, kPersistThreads), ns, 1);
+            e.parts = c.parts;
+            e.nslots = c.key.nslots;
+            e.count = c.key.emit;
+            out.push_back(e);
+        }
+        projection(b->jets + c.first);
+    }
+    PPhase v = new_phase(c, ci, PK_VEL, 0, up(nx, 32), up(ny, 16), up(nz, 4) * ns);
+    v.st = bst(c, c.vel, kVelComp * c.g.NP);
+    v.st.hbar = c.g.hbar;
+    v.st.sharp = 1;
+    out.push_back(v);
+    if (c.key.nslots > 0) {
+        PPhase a = new_phase(c, ci, PK_ADVECT, 0, up(c.key.nslots, kPersistThreads), ns, 1);
+        a.parts = c.parts;
+        a.nslots = c.key.nslots;
+        a.vel = c.vel;
+        a.bs_vel = kVelComp * c.g.NP;
+        a.pow2 = c.g.d_pow2[0] && c.g.d_pow2[1] && c.g.d_pow2[2];
+        a.normw = c.g.norm_w;
+        out.push_back(a);
+    }
+    return true;
+}
+
+// The slot table: the classes' chains interleaved pass by pass, each phase
+// waiting for its predecessor (the class's last phase of the previous step
+// for the first one); `vper_div` divides the virtual CTAs per item.
+int build_plan(isf_batch* b, int vper_div, int blocks_per_sm_cap) {
+    std::vector<std::vector<PPhase>> chains(b->cls.size());
+    for (size_t ci = 0; ci < b->cls.size(); ++ci)
+        if (!class_chain(b, b->cls[ci], (int)ci, chains[ci], b->persist_why))
+            return bfail(b, ISF_ERR_INVALID, b->persist_why);
+    size_t maxlen = 0;
+    for (auto& ch : chains) maxlen = std::max(maxlen, ch.size());
+    std::vector<std::vector<int>> slot_of(chains.size());
+    std::vector<PPhase> ph;
+    for (size_t j = 0; j < maxlen; ++j)
+        for (size_t ci = 0; ci < chains.size(); ++ci)
+            if (j < chains[ci].size()) {
+                slot_of[ci].push_back((int)ph.size());
+                ph.push_back(chains[ci][j]);
+            }
+    for (size_t ci = 0; ci < chains.size(); ++ci)
+        for (size_t j = 0; j < chains[ci].size(); ++j) {
+            PPhase& p = ph[slot_of[ci][j]];
+            p.dep = j > 0 ? slot_of[ci][j - 1] : -1;
+            p.dep_prev = j == 0 ? slot_of[ci].back() : -1;
+        }
+    int smem = 0;
+    std::vector<int> start(1, 0);
+    for (PPhase& p : ph) {
+        p.vblk = persist_vblk(p.kind, p.len);
+        // a virtual CTA is whole warps (its named barrier counts threads in warps)
+        if (p.vblk < 32 || p.vblk % 32 != 0 || p.vblk > kPersistThreads)
+            return bfail(b, ISF_ERR_INVALID, "persistent kernel: pass kind " + std::to_string(p.kind) + " of length " +
+                                                 std::to_string(p.len) + " has no virtual CTA shape");
+        p.smem_v = persist_smem(p.kind, p.len);
+        const int vmax = std::max(1, kPersistThreads / p.vblk);
+        p.vper = std::max(1, vmax / vper_div);
+        p.items = (p.tiles + p.vper - 1) / p.vper;
+        smem = std::max(smem, p.vper * p.smem_v);
+        start.push_back(start.back() + p.items);
+    }
+    int bps = 0, sms = 0;
+    B_CUDA(b, persist_setup(smem, &bps), "persistent kernel set-up");
+    B_CUDA(b, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "persistent kernel set-up");
+    if (bps < 1) return bfail(b, ISF_ERR_INVALID, "persistent kernel: no block fits an SM");
+    bps = std::min(bps, blocks_per_sm_cap);
+    free_persist(b);
+    if (cudaMalloc(&b->d_ph, sizeof(PPhase) * ph.size()) != cudaSuccess ||
+        cudaMalloc(&b->d_slot, sizeof(int) * start.size()) != cudaSuccess ||
+        cudaMalloc(&b->d_ctl, 2 * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&b->d_status, 4 * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, ISF_ERR_NOMEM, "persistent kernel: device allocation failed");
+    }
+    B_CUDA(b, cudaMemcpy(b->d_ph, ph.data(), sizeof(PPhase) * ph.size(), cudaMemcpyHostToDevice), "persistent plan");
+    B_CUDA(b, cudaMemcpy(b->d_slot, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice), "persistent plan");
+    B_CUDA(b, cudaMemset(b->d_status, 0, 4 * sizeof(int)), "persistent plan");
+    b->phases = ph;
+    b->slot_start = start;
+    b->psmem = smem;
+    b->pgrid = sms * bps;
+    b->pvper_div = vper_div;
+    return ISF_OK;
+}
+
+PPlan make_plan(const isf_batch* b, int nsteps) {
+    PPlan p;
+    std::memset(&p, 0, sizeof(p));
+    p.ph = b->d_ph;
+    p.slot_start = b->d_slot;
+    p.nslot = (int)b->phases.size();
+    p.items_per_step = b->slot_start.back();
+    p.nsteps = nsteps;
+    p.done = b->d_done;
+    p.ctl = b->d_ctl;
+    p.status = b->d_status;
+    p.spin_limit = b->spin_limit;
+    p.stall = (b->mode & ISF_PERSIST_STALL) ? 1 : 0;
+    p.step = b->step;
+    p.rt = b->rt;
+    p.jets = b->jets;
+    p.emits = b->emits;
+    p.counters = b->counters;
+    return p;
+}
+
+// queue nsteps persistent steps on s: zero the item counters, one launch
+cudaError_t queue_persist(isf_batch* b, int nsteps, cudaStream_t s) {
+    const size_t nslot = b->phases.size();
+    cudaError_t e = cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * nslot * nsteps, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctl, 0, 2 * sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, 4 * sizeof(int), s);
+    if (e == cudaSuccess) e = launch_persist(make_plan(b, nsteps), b->pgrid, b->psmem, s);
+    return e;
+}
+
+int ensure_done(isf_batch* b, long long nsteps) {
+    if (b->done_cap >= nsteps) return ISF_OK;
+    for (auto& kv : b->pgraphs) cudaGraphExecDestroy(kv.second);
+    b->pgraphs.clear();
+    cudaFree(b->d_done);
+    b->d_done = nullptr;
+    b->done_cap = 0;
+    const long long cap = std::max<long long>(nsteps, 128);
+    if (cudaMalloc(&b->d_done, sizeof(unsigned) * b->phases.size() * cap) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, ISF_ERR_NOMEM, "persistent kernel: device allocation failed");
+    }
+    b->done_cap = cap;
+    return ISF_OK;
+}
+
+// The persistent kernel's tile autotuner: virtual CTAs per work item (all
+// that fit a block, or half of them) and blocks per SM (as many as fit, or
+// one), each timed over 3 steps of the zeroed state; keeps the fastest.
+int tune_persist(isf_batch* b, bool tune) {
+    int best_div = 1, best_bps = 2;
+    if (tune) {
+        cudaEvent_t e0, e1;
+        B_CUDA(b, cudaEventCreate(&e0), "persistent tuning");
+        B_CUDA(b, cudaEventCreate(&e1), "persistent tuning");
+        float best = 1e30f;
+        int rc = ISF_OK;
+        for (int div : {1, 2}) {
+            for (int bps : {2, 1}) {
+                if ((rc = build_plan(b, div, bps)) != ISF_OK) break;
+                if ((rc = ensure_done(b, 3)) != ISF_OK) break;
+                cudaError_t e = queue_persist(b, 3, b->stream);  // warm-up
+                if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+                if (e == cudaSuccess) e = queue_persist(b, 3, b->stream);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                int st = 0;
+                if (e == cudaSuccess) e = cudaMemcpy(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) {
+                    rc = bcuda(b, e, "persistent kernel tuning");
+                    break;
+                }
+                if (st != 0) {
+                    rc = bfail(b, ISF_ERR_TIMEOUT, "persistent kernel tuning: a device-side wait ran out");
+                    break;
+                }
+                if (ms < best * 0.97f) {
+                    best = ms;
+                    best_div = div;
+                    best_bps = bps;
+                }
+            }
+            if (rc != ISF_OK) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc != ISF_OK) return rc;
+    }
+    if (int rc = build_plan(b, best_div, best_bps)) return rc;
+    return ensure_done(b, 1);
 }
 
 int sim_ok(isf_batch* b, int32_t sim, const char* who) {
@@ -566,6 +851,28 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
         e = clear(c);
         if (e != cudaSuccess) return fail_free(ISF_ERR_CUDA, std::string("isf_batch_create: clear: ") + cudaGetErrorString(e));
     }
+    // the persistent kernel's plan and tiles, when every class fits it (the
+    // tuning runs in place on the cleared state: clear again after it)
+    {
+        std::vector<PPhase> probe;
+        std::string pwhy;
+        b->persist_ok = true;
+        for (size_t ci = 0; ci < b->cls.size() && b->persist_ok; ++ci)
+            b->persist_ok = class_chain(b, b->cls[ci], (int)ci, probe, pwhy);
+        b->persist_why = pwhy;
+    }
+    if (b->persist_ok && e == cudaSuccess) {
+        e = cudaStreamSynchronize(b->stream);
+        const int rc = e == cudaSuccess ? tune_persist(b, tune != 0) : ISF_OK;
+        if (rc != ISF_OK) {
+            const std::string m = b->err;
+            free_batch(b);
+            return bfail(nullptr, rc, "isf_batch_create: " + m);
+        }
+        for (BatchClass& c : b->cls)
+            if (e == cudaSuccess) e = clear(c);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->step, 0, sizeof(long long), b->stream);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(b->counters, 0, sizeof(unsigned long long) * kCounterStride * nsims, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return fail_free(ISF_ERR_CUDA, std::string("isf_batch_create: ") + cudaGetErrorString(e));
@@ -654,6 +961,29 @@ int isf_batch_init_jet(isf_batch* b, int32_t iters) {
 int isf_batch_step(isf_batch* b, int32_t nsteps) {
     B_ENTER(b);
     if (nsteps < 0) return bfail(b, ISF_ERR_INVALID, "isf_batch_step: nsteps must be >= 0");
+    if (b->mode & ISF_PERSIST_ON) {
+        if (nsteps == 0) return ISF_OK;
+        if (int rc = ensure_done(b, nsteps)) return rc;
+        auto it = b->pgraphs.find(nsteps);
+        if (it == b->pgraphs.end()) {
+            // one graph per step count: zero the counters, one persistent launch
+            B_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "isf_batch_step: capture");
+            const cudaError_t e = queue_persist(b, nsteps, b->stream);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+            cudaGraphExec_t exec = nullptr;
+            cudaError_t e3 = e != cudaSuccess ? e : e2;
+            if (e3 == cudaSuccess) e3 = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e3 != cudaSuccess) {
+                cudaGetLastError();
+                return bcuda(b, e3, "isf_batch_step: capturing the persistent launch");
+            }
+            it = b->pgraphs.emplace(nsteps, exec).first;
+        }
+        B_CUDA(b, cudaGraphLaunch(it->second, b->stream), "isf_batch_step: cudaGraphLaunch");
+        return ISF_OK;
+    }
     if (int rc = capture_step(b)) return rc;
     for (int i = 0; i < nsteps; ++i) B_CUDA(b, cudaGraphLaunch(b->exec, b->stream), "isf_batch_step: cudaGraphLaunch");
     return ISF_OK;
@@ -677,6 +1007,33 @@ int isf_batch_get_stream(const isf_batch* b, void** stream) {
 int isf_batch_sync(isf_batch* b) {
     B_ENTER(b);
     B_CUDA(b, cudaStreamSynchronize(b->stream), "isf_batch_sync");
+    if (b->d_status) {
+        int st[3] = {0, 0, 0};
+        B_CUDA(b, cudaMemcpy(st, b->d_status, sizeof(st), cudaMemcpyDeviceToHost), "isf_batch_sync: status");
+        if (st[0] != 0) {
+            const int slot = std::max(0, std::min(st[1], (int)b->phases.size() - 1));
+            const PPhase& p = b->phases[(size_t)slot];
+            return bfail(b, st[0], "isf_batch_sync: a device-side wait of the persistent kernel ran out (slot " +
+                                       std::to_string(st[1]) + ": pass kind " + std::to_string(p.kind) + " of class " +
+                                       std::to_string(p.cls) + ", step " + std::to_string(st[2]) +
+                                       " of the launch); the ensemble state is partly stepped");
+        }
+    }
+    return ISF_OK;
+}
+
+int isf_batch_set_persistent(isf_batch* b, int32_t mode, int64_t spin_limit) {
+    B_ENTER(b);
+    if (mode & ~(ISF_PERSIST_ON | ISF_PERSIST_STALL))
+        return bfail(b, ISF_ERR_INVALID, "isf_batch_set_persistent: unknown mode bits");
+    if ((mode & ISF_PERSIST_ON) && !b->persist_ok)
+        return bfail(b, ISF_ERR_INVALID, "isf_batch_set_persistent: " + b->persist_why);
+    B_CUDA(b, cudaStreamSynchronize(b->stream), "isf_batch_set_persistent");
+    b->mode = mode;
+    b->spin_limit = spin_limit > 0 ? spin_limit : (1LL << 22);
+    for (auto& kv : b->pgraphs) cudaGraphExecDestroy(kv.second);
+    b->pgraphs.clear();
+    if (b->d_status) B_CUDA(b, cudaMemset(b->d_status, 0, 4 * sizeof(int)), "isf_batch_set_persistent");
     return ISF_OK;
 }
 

@@ -1,0 +1,308 @@
+// The persistent batch kernel (see isf_persist.h): K ensemble steps in one
+// launch, the pass bodies of the single-simulation kernels run as virtual
+// CTAs of a 256-thread block, dependencies between passes as bounded waits.
+#include <type_traits>
+
+#include "isf_particles.cuh"
+#include "isf_persist.h"
+#include "isf_stencil.cuh"
+
+namespace isf {
+
+namespace {
+
+// x pencil lengths and (y, z) plane sizes the kernel is instantiated for;
+// every one gives virtual CTAs of whole warps (the named barriers count
+// threads in warps)
+template <class F>
+__device__ __forceinline__ void with_xlen(int n, const F& f) {
+    switch (n) {
+        case 16: f(std::integral_constant<int, 16>()); break;
+        case 32: f(std::integral_constant<int, 32>()); break;
+        case 48: f(std::integral_constant<int, 48>()); break;
+        case 64: f(std::integral_constant<int, 64>()); break;
+        case 96: f(std::integral_constant<int, 96>()); break;
+        case 128: f(std::integral_constant<int, 128>()); break;
+        default: break;
+    }
+}
+template <class F>
+__device__ __forceinline__ void with_plane(int n, const F& f) {
+    switch (n) {
+        case 32: f(std::integral_constant<int, 32>()); break;
+        case 48: f(std::integral_constant<int, 48>()); break;
+        case 64: f(std::integral_constant<int, 64>()); break;
+        case 96: f(std::integral_constant<int, 96>()); break;
+        default: break;
+    }
+}
+
+template <int N>
+using PShape = PlaneShape<N, kPersistThreads>;
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Poll *p until it reaches need, at most limit times; false if the limit ran
+// out or another block reported an error.
+__device__ bool bounded_wait(const unsigned* p, unsigned need, long long limit, const int* status) {
+    for (long long k = 0;; ++k) {
+        if (ld_relaxed(p) >= need) return true;
+        if (ld_relaxed(status) != 0 || k >= limit) return false;
+        __nanosleep(k < 64 ? 32 : 256);
+    }
+}
+
+__device__ void report(const PPlan& P, int slot, int step) {
+    if (atomicCAS(&P.status[0], 0, ISF_ERR_TIMEOUT) == 0) {
+        P.status[1] = slot;
+        P.status[2] = step;
+    }
+    __threadfence();
+}
+
+// one tile (virtual CTA) of a phase
+__device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int tile, int step, int vt,
+                                         unsigned char* sm, const NamedBar& bar) {
+    Blk bk;
+    bk.x = tile % ph.gx;
+    bk.y = (tile / ph.gx) % ph.gy;
+    bk.z = tile / (ph.gx * ph.gy);
+    bk.tid = vt;
+    switch (ph.kind) {
+        case PK_PROLOGUE: {
+            // the step-graph prologue of isf_batch.cu for this class's simulations
+            const long long it = *P.step + step + 1;
+            for (int s = vt; s < ph.nsim; s += ph.vblk) {
+                const int i = ph.first + s;
+                const SimRT r = P.rt[i];
+                P.jets[i].omgterm = __fmul_rn(r.omega, __fmul_rn((float)it, r.dt));
+                P.emits[i].e.counter = (uint64_t)it;
+                P.emits[i].start = r.nslots > 0 ? ((it - 1) * r.count) % r.nslots : 0;
+            }
+            break;
+        }
+        case PK_X_FWD:
+            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_FWD, 1>(ph.x, bk, sm, bar); });
+            break;
+        case PK_X_INV_NORM:
+            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_INV_NORM, 1>(ph.x, bk, sm, bar); });
+            break;
+        case PK_Y_FWD:
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_FWD, 1>(ph.yz, bk, sm, bar); });
+            break;
+        case PK_Z_MASK:
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_MASK, 1>(ph.yz, bk, sm, bar); });
+            break;
+        case PK_Y_INV:
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_INV, 1>(ph.yz, bk, sm, bar); });
+            break;
+        case PK_XR_FWD:
+            with_xlen(ph.len, [&](auto n) { xreal_body<decltype(n)::value, XR_FWD, 1, true>(ph.x, bk, sm, bar); });
+            break;
+        case PK_XR_INV_GAUGE:
+            with_xlen(ph.len,
+                      [&](auto n) { xreal_body<decltype(n)::value, XR_INV_GAUGE, 1, true>(ph.x, bk, sm, bar); });
+            break;
+        case PK_PLANE:
+            with_plane(ph.len, [&](auto n) {
+                constexpr int N = decltype(n)::value;
+                plane_body<N, PShape<N>>(ph.pl, bk, sm, bar);
+            });
+            break;
+        case PK_DIV:
+            stencil_body<ST_DIV>(ph.st, bk, *reinterpret_cast<StencilSmem*>(sm), bar);
+            break;
+        case PK_VEL:
+            stencil_body<ST_VEL>(ph.st, bk, *reinterpret_cast<StencilSmem*>(sm), bar);
+            break;
+        case PK_EMIT: {
+            const long long j = (long long)bk.x * ph.vblk + vt;
+            if (j < ph.count) {
+                const EmitState& st = P.emits[ph.first + bk.y];
+                const float3 p = emit_point(j, st.e);
+                const long long s = (st.start + j) % ph.nslots;
+                float* parts = ph.parts + bk.y * 3 * ph.nslots;
+                parts[3 * s + 0] = p.x;
+                parts[3 * s + 1] = p.y;
+                parts[3 * s + 2] = p.z;
+            }
+            break;
+        }
+        case PK_ADVECT: {
+            const long long k = (long long)bk.x * ph.vblk + vt;
+            unsigned clamps = 0, live = 0;
+            if (k < ph.nslots) {
+                const AdvConst kc = adv_const(ph.g, ph.vel + bk.y * ph.bs_vel);
+                const float dt = ph.g.dt, s6 = ph.g.dt / 6.0f;
+                float* parts = ph.parts + bk.y * 3 * ph.nslots;
+                if (ph.normw) {
+                    if (ph.pow2)
+                        advect_slot<true, true, NamedBar>(kc, parts, (int)k, dt, s6, clamps, live, nullptr);
+                    else
+                        advect_slot<false, true, NamedBar>(kc, parts, (int)k, dt, s6, clamps, live, nullptr);
+                } else {
+                    if (ph.pow2)
+                        advect_slot<true, false, NamedBar>(kc, parts, (int)k, dt, s6, clamps, live, nullptr);
+                    else
+                        advect_slot<false, false, NamedBar>(kc, parts, (int)k, dt, s6, clamps, live, nullptr);
+                }
+            }
+            // warp-aggregated counters (a virtual CTA is whole warps)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                clamps += __shfl_down_sync(0xffffffffu, clamps, o);
+                live += __shfl_down_sync(0xffffffffu, live, o);
+            }
+            if ((vt & 31) == 0) {
+                unsigned long long* c = P.counters + (size_t)(ph.first + bk.y) * kCounterStride;
+                if (clamps) atomicAdd(&c[0], (unsigned long long)clamps);
+                if (live) atomicAdd(&c[1], (unsigned long long)live);
+            }
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int s_item, s_go;
+    const int total = P.items_per_step * P.nsteps;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int it = -1;
+            if (ld_relaxed(&P.status[0]) == 0) {
+                it = (int)atomicAdd(&P.ctl[0], 1u);
+                if (it >= total) it = -1;
+            }
+            s_item = it;
+        }
+        __syncthreads();
+        const int it = s_item;
+        if (it < 0) break;
+        const int step = it / P.items_per_step, r = it - step * P.items_per_step;
+        int slot = 0;
+        while (P.slot_start[slot + 1] <= r) ++slot;
+        const PPhase& ph = P.ph[slot];
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (ph.dep >= 0)
+                ok = bounded_wait(&P.done[step * P.nslot + ph.dep], (unsigned)P.ph[ph.dep].items, P.spin_limit,
+                                  P.status);
+            if (ok && step > 0 && ph.dep_prev >= 0)
+                ok = bounded_wait(&P.done[(step - 1) * P.nslot + ph.dep_prev], (unsigned)P.ph[ph.dep_prev].items,
+                                  P.spin_limit, P.status);
+            // the stall switch: an item with a dependency also waits for
+            // status[3], which nothing writes, so the wait runs out
+            if (ok && P.stall && (ph.dep >= 0 || (step > 0 && ph.dep_prev >= 0)))
+                ok = bounded_wait(reinterpret_cast<const unsigned*>(&P.status[3]), 1u, P.spin_limit, P.status);
+            if (!ok) report(P, slot, step);
+            __threadfence();  // acquire: this item's reads see the predecessor's writes
+            s_go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_go) break;
+        const int v = threadIdx.x / ph.vblk;
+        const int tile = (r - P.slot_start[slot]) * ph.vper + v;
+        if (v < ph.vper && tile < ph.tiles)
+            run_tile(P, ph, tile, step, threadIdx.x - v * ph.vblk, smraw + v * ph.smem_v, NamedBar{1 + v, ph.vblk});
+        __syncthreads();  // every virtual CTA of the item is done
+        if (threadIdx.x == 0) {
+            __threadfence();  // release: the item's writes before its count
+            atomicAdd(&P.done[step * P.nslot + slot], 1u);
+            // the last item of the launch advances the ensemble's step counter
+            if (atomicAdd(&P.ctl[1], 1u) + 1 == (unsigned)total) *P.step += P.nsteps;
+        }
+    }
+}
+
+bool persist_len_ok(int n) {
+    switch (n) {
+        case 16: case 32: case 48: case 64: case 96: case 128: return true;
+        default: return false;
+    }
+}
+
+bool persist_plane_ok(int n) { return n == 32 || n == 48 || n == 64 || n == 96; }
+
+namespace {
+template <class F>
+int host_xlen(int n, const F& f) {
+    switch (n) {
+        case 16: return f(std::integral_constant<int, 16>());
+        case 32: return f(std::integral_constant<int, 32>());
+        case 48: return f(std::integral_constant<int, 48>());
+        case 64: return f(std::integral_constant<int, 64>());
+        case 96: return f(std::integral_constant<int, 96>());
+        case 128: return f(std::integral_constant<int, 128>());
+        default: return 0;
+    }
+}
+template <class F>
+int host_plane(int n, const F& f) {
+    switch (n) {
+        case 32: return f(std::integral_constant<int, 32>());
+        case 48: return f(std::integral_constant<int, 48>());
+        case 64: return f(std::integral_constant<int, 64>());
+        case 96: return f(std::integral_constant<int, 96>());
+        default: return 0;
+    }
+}
+}  // namespace
+
+int persist_vblk(int kind, int len) {
+    switch (kind) {
+        case PK_X_FWD: case PK_X_INV_NORM:
+            return host_xlen(len, [](auto n) { return XShape<decltype(n)::value, X_PSI_FWD, 1>::BLK; });
+        case PK_Y_FWD: case PK_Z_MASK: case PK_Y_INV:
+            return host_plane(len, [](auto n) { return YZShape<decltype(n)::value, float4, YZ_FWD, 1>::BLK; });
+        case PK_XR_FWD: case PK_XR_INV_GAUGE:
+            return host_xlen(len, [](auto n) { return XRShape<decltype(n)::value, 1, true>::BLK; });
+        case PK_PLANE:
+            return host_plane(len, [](auto n) { return PlaneShape<decltype(n)::value, kPersistThreads>::BLK; });
+        default:
+            return kPersistThreads;
+    }
+}
+
+int persist_smem(int kind, int len) {
+    switch (kind) {
+        case PK_X_FWD: case PK_X_INV_NORM:
+            return host_xlen(len, [](auto n) { return (int)XShape<decltype(n)::value, X_PSI_FWD, 1>::SMEM; });
+        case PK_Y_FWD: case PK_Z_MASK: case PK_Y_INV:
+            return host_plane(len, [](auto n) { return (int)YZShape<decltype(n)::value, float4, YZ_FWD, 1>::SMEM; });
+        case PK_XR_FWD: case PK_XR_INV_GAUGE:
+            return host_xlen(len, [](auto n) { return (int)XRShape<decltype(n)::value, 1, true>::SMEM; });
+        case PK_PLANE:
+            return host_plane(len, [](auto n) { return (int)PlaneShape<decltype(n)::value, kPersistThreads>::SMEM; });
+        case PK_DIV: case PK_VEL:
+            return (int)sizeof(StencilSmem);
+        default:
+            return 0;
+    }
+}
+
+cudaError_t persist_setup(int smem_bytes, int* blocks_per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_persist, kPersistThreads, smem_bytes);
+}
+
+cudaError_t launch_persist(const PPlan& p, int grid, int smem_bytes, cudaStream_t s) {
+    k_persist<<<grid, kPersistThreads, smem_bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace isf

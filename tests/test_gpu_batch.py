@@ -176,3 +176,70 @@ def test_batch_errors(isfpkg, cfgs):
         b.set_psi(0, cuda(psi0[2]))   # wrong shape
     with pytest.raises(isfpkg.ISFError, match="nsteps"):
         b.step(-1)
+
+
+def persistent_run(isfpkg, sims, psi0, parts0, init_iters, chunks, tune=True):
+    b = isfpkg.ISFBatch(sims, tune=tune)
+    b.set_persistent(True)
+    for i in range(len(sims)):
+        b.set_psi(i, cuda(psi0[i]))
+        b.set_particles(i, cuda(parts0[i]))
+    b.init_jet(init_iters)
+    for k in chunks:
+        b.step(k)
+    b.sync()
+    return b
+
+
+def test_persistent_batch_equals_plain_runs_bitwise(isfpkg, cfgs):
+    """All steps of a call in one launch of the persistent kernel (passes as
+    work items with bounded device-side waits between them): bit for bit the
+    single-simulation isf_step runs, across two calls (4 + 2 steps)."""
+    sims, psi0, parts0 = small_ensemble(cfgs)
+    b = persistent_run(isfpkg, sims, psi0, parts0, 10, (4, 2))
+    for i, s in enumerate(sims):
+        psi, parts = plain_run(isfpkg, s, psi0[i], parts0[i], 10, 6)
+        assert torch.equal(b.psi(i), psi), i
+        assert torch.equal(b.particles(i), parts), i
+    live = b.counters(4)["live"]
+    assert 0 < live <= 300 * 6 * 7 // 2
+
+
+def test_persistent_wait_times_out_and_the_gpu_keeps_answering(isfpkg, cfgs):
+    """A wait that cannot be satisfied (stall: dependent passes also wait for
+    a flag that nothing sets) runs out after spin_limit polls: the kernel
+    reports ISF_ERR_TIMEOUT through its status word, every block stops, and
+    sync raises.  The context stays usable: the same batch, reset and
+    stepped again without the stall, matches a graph-mode batch bitwise."""
+    sims, psi0, parts0 = small_ensemble(cfgs)
+    b = isfpkg.ISFBatch(sims, tune=False)
+    for i in range(len(sims)):
+        b.set_psi(i, cuda(psi0[i]))
+        b.set_particles(i, cuda(parts0[i]))
+    b.set_persistent(True, spin_limit=2000, stall=True)
+    b.step(3)
+    with pytest.raises(isfpkg.ISFError) as err:
+        b.sync()
+    assert err.value.code == isfpkg._lib.ISF_ERR_TIMEOUT
+    assert "ran out" in str(err.value)
+    b.set_persistent(True)
+    b.set_step(0)
+    for i in range(len(sims)):
+        b.set_psi(i, cuda(psi0[i]))
+        b.set_particles(i, cuda(parts0[i]))
+    b.init_jet(2)
+    b.step(3)
+    b.sync()
+    ref = batch_run(isfpkg, sims, psi0, parts0, 2, 3, tune=False)
+    for i in range(len(sims)):
+        assert torch.equal(b.psi(i), ref.psi(i)), i
+        assert torch.equal(b.particles(i), ref.particles(i)), i
+
+
+def test_persistent_rejects_grids_it_is_not_built_for(isfpkg, cfgs):
+    sims, _, _ = cfgs.ensemble(nsims=2, seed=3, nslots=64)
+    sims[1]["dims"], sims[1]["physical_size"] = (64, 32, 16), (4, 2, 1)   # ny != nz: no plane solver
+    b = isfpkg.ISFBatch(sims, tune=False)
+    with pytest.raises(isfpkg.ISFError, match="persistent kernel needs"):
+        b.set_persistent(True)
+    b.close()
