@@ -18,9 +18,11 @@
  *   - All work is asynchronous on the handle's stream until isf_sync(), like
  *     GPUArrays' launches (examples/benchmark.jl:66).  A handle is not
  *     thread-safe; separate handles are independent.
- *   - Grid sizes: each of nx, ny, nz in {8,12,16,24,32,48,64,96,128,192,256,
- *     384,512}, nx a multiple of 16, ny*nz a multiple of 32 (ISF_ERR_INVALID
- *     otherwise); psi pointers 16-byte aligned, complex arrays 8-byte aligned.
+ *   - Grid sizes: each of nx, ny, nz in {8,12,16,20,24,32,40,48,50,56,64,80,
+ *     96,100,112,128,160,192,200,256,384,512} (the FFT's radix plans: 2^a 3^b
+ *     up to 512, and lengths with a factor 5 or 7; ISF_ERR_INVALID otherwise);
+ *     the reference takes any dims (src/parallel.jl:41-79).  psi pointers
+ *     16-byte aligned, complex arrays 8-byte aligned.
  */
 #ifndef ISF_H
 #define ISF_H

@@ -28,7 +28,7 @@
  * oracle/matlabport.py and compared in tests/test_oracle_cpu.py).
  *
  * FFT: FFTW / CLFFT (third-party, unpinned, not in the reference tree) are
- * replaced by a self-written recursive mixed-radix (2,3,4) decimation-in-time
+ * replaced by a self-written recursive mixed-radix (2,3,4,5,7) decimation-in-time
  * DFT with the AbstractFFTs conventions the reference relies on: forward
  * exp(-2 pi i jk/n) unnormalised, inverse exp(+2 pi i jk/n) scaled by 1/N.
  * It is checked against numpy.fft in FP64.
@@ -75,6 +75,8 @@ struct Plan1D {
         while (m % 4 == 0) { radix.push_back(4); m /= 4; }
         while (m % 2 == 0) { radix.push_back(2); m /= 2; }
         while (m % 3 == 0) { radix.push_back(3); m /= 3; }
+        while (m % 5 == 0) { radix.push_back(5); m /= 5; }
+        while (m % 7 == 0) { radix.push_back(7); m /= 7; }
         tw.resize(n);
         for (int j = 0; j < n; ++j) {
             long double a = -2.0L * (long double)kPi * (long double)j / (long double)n;
@@ -98,7 +100,7 @@ struct Plan1D {
         for (int q = 0; q < r; ++q) rec(in + q * is, is * r, out + q * m, m, stage + 1, sign);
         const long step = n / len;  // W_len^j = tw[j * step]
         for (int k = 0; k < m; ++k) {
-            C t[4];
+            C t[7];
             for (int q = 0; q < r; ++q) {
                 C v = out[q * m + k];
                 t[q] = (q == 0 || k == 0) ? v : v * W((long)q * k * step, sign);
@@ -114,6 +116,14 @@ struct Plan1D {
                 out[k + m] = b + e;
                 out[k + 2 * m] = a - c;
                 out[k + 3 * m] = b - e;
+            } else if (r == 5 || r == 7) {
+                // y_s = sum_q t_q w^{qs}, w = exp(sign 2 pi i / r) = W(n / r) (direct DFT)
+                const long wr = n / r;
+                for (int s = 0; s < r; ++s) {
+                    C acc = t[0];
+                    for (int q = 1; q < r; ++q) acc += t[q] * W((long)((q * s) % r) * wr, sign);
+                    out[k + s * m] = acc;
+                }
             } else {  // r == 3
                 const R h = (R)0.866025403784438646763723170752936183L;  // sin(pi/3)
                 C s = t[1] + t[2], dd = t[1] - t[2];

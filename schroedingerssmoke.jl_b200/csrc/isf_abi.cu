@@ -98,17 +98,9 @@ bool valid_grid(const int n[3], std::string& why) {
     for (int a = 0; a < 3; ++a) {
         if (!supported_len(n[a])) {
             why = "grid_res[" + std::to_string(a) + "] = " + std::to_string(n[a]) +
-                  " is not one of 8,12,16,24,32,48,64,96,128,192,256,384,512";
+                  " is not one of 8,12,16,20,24,32,40,48,50,56,64,80,96,100,112,128,160,192,200,256,384,512";
             return false;
         }
-    }
-    if (n[0] % 16 != 0) {
-        why = "grid_res[0] must be a multiple of 16";
-        return false;
-    }
-    if (((long long)n[1] * n[2]) % 32 != 0) {
-        why = "grid_res[1]*grid_res[2] must be a multiple of 32";
-        return false;
     }
     return true;
 }

@@ -289,6 +289,7 @@ int kind_len(const BatchClass& c, int kind) {
 
 // a G is a candidate when the kernels exist for it and it divides the work
 bool tile_fits(const BatchClass& c, int kind, int G) {
+    if (G == 1) return true;  // single-group tiles guard a partial last tile
     if (!grouped_tile_ok(kind_len(c, kind), G)) return false;
     // a k-major class runs its real x passes ungrouped and has no half-spectrum y / z passes
     if (c.kmajor && (kind == ISF_TILE_X_REAL || kind == ISF_TILE_Y_HALF || kind == ISF_TILE_Z_HALF)) return G == 1;

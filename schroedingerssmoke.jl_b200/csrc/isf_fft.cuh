@@ -83,11 +83,68 @@ __device__ __forceinline__ void dft8(T* x) {
     x[7] = csub(e3, o3);
 }
 
+// Odd prime radix R = 2M + 1 from the symmetric pairs a_q = x_q + x_{R-q},
+// b_q = x_q - x_{R-q} (q = 1..M):
+//   y_k     = x_0 + sum_q cos(2 pi q k / R) a_q + S i sum_q sin(2 pi q k / R) b_q
+//   y_{R-k} = x_0 + sum_q cos(2 pi q k / R) a_q - S i sum_q sin(2 pi q k / R) b_q
+// for k = 1..M, with cos / sin of 2 pi m / R taken from the first M angles by
+// the symmetries of m mod R.
+template <int R, int S, class T>
+__device__ __forceinline__ void dft_odd(T* x, const float* c, const float* sn) {
+    constexpr int M = R / 2;
+    T a[M], b[M];
+#pragma unroll
+    for (int q = 1; q <= M; ++q) {
+        a[q - 1] = cadd(x[q], x[R - q]);
+        b[q - 1] = csub(x[q], x[R - q]);
+    }
+    T y0 = x[0];
+#pragma unroll
+    for (int q = 0; q < M; ++q) y0 = cadd(y0, a[q]);
+    T yk[R];
+#pragma unroll
+    for (int k = 1; k <= M; ++k) {
+        T re = x[0], im = cscale(b[0], 0.f);
+#pragma unroll
+        for (int q = 1; q <= M; ++q) {
+            const int m = (q * k) % R;                 // angle 2 pi m / R
+            const int mm = m <= M ? m : R - m;         // cos(2 pi m / R) = c[mm - 1]
+            const float sg = m <= M ? 1.f : -1.f;      // sin(2 pi m / R) = sg * sn[mm - 1]
+            re = cadd(re, cscale(a[q - 1], c[mm - 1]));
+            im = cadd(im, cscale(b[q - 1], sg * sn[mm - 1]));
+        }
+        const T u = mul_si<S>(im);
+        yk[k] = cadd(re, u);
+        yk[R - k] = csub(re, u);
+    }
+    x[0] = y0;
+#pragma unroll
+    for (int k = 1; k < R; ++k) x[k] = yk[k];
+}
+
+template <int S, class T>
+__device__ __forceinline__ void dft5(T* x) {
+    // cos / sin of 2 pi / 5 and 4 pi / 5
+    const float c[2] = {0.30901699437494742f, -0.80901699437494742f};
+    const float sn[2] = {0.95105651629515357f, 0.58778525229247313f};
+    dft_odd<5, S>(x, c, sn);
+}
+
+template <int S, class T>
+__device__ __forceinline__ void dft7(T* x) {
+    // cos / sin of 2 pi k / 7, k = 1, 2, 3
+    const float c[3] = {0.62348980185873353f, -0.22252093395631440f, -0.90096886790241913f};
+    const float sn[3] = {0.78183148246802981f, 0.97492791218182361f, 0.43388373911755812f};
+    dft_odd<7, S>(x, c, sn);
+}
+
 template <int R, int S, class T>
 __device__ __forceinline__ void dft(T* x) {
     if constexpr (R == 2) dft2<S>(x[0], x[1]);
     else if constexpr (R == 3) dft3<S>(x[0], x[1], x[2]);
     else if constexpr (R == 4) dft4<S>(x[0], x[1], x[2], x[3]);
+    else if constexpr (R == 5) dft5<S>(x);
+    else if constexpr (R == 7) dft7<S>(x);
     else if constexpr (R == 8) dft8<S>(x);
     else static_assert(R == 2, "unsupported radix");
 }
@@ -208,7 +265,8 @@ constexpr int isf_emax(int N, int NT, std::initializer_list<int> rs) {
 
 #define ISF_UNPAREN(...) __VA_ARGS__
 
-// Supported pencil lengths: 2^a 3^b, 8 <= N <= 512.  NT = N / (first radix).
+// Supported pencil lengths: 2^a 3^b with 8 <= N <= 512, and 20, 40, 50, 56,
+// 80, 100, 112, 160, 200 (radices 5 and 7).  NT = N / (first radix).
 // FWD lists the radices in stage order, REV the same radices reversed (the
 // inverse of run_spectral).
 template <int N>
@@ -261,6 +319,16 @@ ISF_PLAN(192, 8, (8, 8, 3), (3, 8, 8))
 ISF_PLAN(256, 8, (8, 8, 4), (4, 8, 8))
 ISF_PLAN(384, 8, (8, 4, 4, 3), (3, 4, 4, 8))
 ISF_PLAN(512, 8, (8, 8, 8), (8, 8, 8))
+// lengths with factors 5 and 7
+ISF_PLAN(20, 4, (4, 5), (5, 4))
+ISF_PLAN(40, 8, (8, 5), (5, 8))
+ISF_PLAN(50, 5, (5, 5, 2), (2, 5, 5))
+ISF_PLAN(56, 8, (8, 7), (7, 8))
+ISF_PLAN(80, 4, (4, 4, 5), (5, 4, 4))
+ISF_PLAN(100, 4, (4, 5, 5), (5, 5, 4))
+ISF_PLAN(112, 4, (4, 4, 7), (7, 4, 4))
+ISF_PLAN(160, 8, (8, 4, 5), (5, 4, 8))
+ISF_PLAN(200, 8, (8, 5, 5), (5, 5, 8))
 #undef ISF_PLAN
 
 }  // namespace isf

@@ -81,11 +81,15 @@ __device__ __forceinline__ void xpass_body(const XArgs& a, const Blk& bk, unsign
     const int t = lt % NT, q = lt / NT;
     const long long row = ((long long)bk.x * G + grp) * C + q;
     const long long rb = row * N;
+    // the last CTA of a grid whose row count is not a multiple of C holds
+    // pencils past the end: they read zeros and store nothing
+    const bool valid = row < (long long)a.g.n[1] * a.g.n[2];
     float4* __restrict__ psi = a.psi + bk.y * a.bs_psi;
     float2* __restrict__ F = a.F + bk.y * a.bs_F;
     T x[Plan<N>::EMAX];
 
     auto src = [&](int j) -> T {
+        if (!valid) return T{};
         if constexpr (Tr::psi_elems) {
             return psi[rb + j];
         } else {
@@ -93,6 +97,7 @@ __device__ __forceinline__ void xpass_body(const XArgs& a, const Blk& bk, unsign
         }
     };
     auto dst = [&](int j, const T& v) {
+        if (!valid) return;
         if constexpr (OP == X_PSI_FWD || OP == X_PSI_INV) {
             psi[rb + j] = v;
         } else if constexpr (OP == X_PSI_INV_NORM) {
@@ -156,10 +161,16 @@ __device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsign
     const int sim = bk.y;
     float2* __restrict__ Fs = a.F + sim * a.bs_F;
     T x[Plan<N>::EMAX];
+    // row pairs past the last row (a row count that is not a multiple of
+    // 2 C) read zeros and store nothing; the k-major layout has none
+    const long long rows = (long long)ny * nz;
+    const bool v0 = KM || r0 < rows, v1 = KM || r0 + 1 < rows;
     if constexpr (OP == XR_FWD) {
         const float* __restrict__ f0 = a.rin + sim * a.bs_r + r0 * N;
         const float* __restrict__ f1 = f0 + N;
-        auto src = [&](int j) -> T { return make_float2(ldm<BarT>(&f0[j]), ldm<BarT>(&f1[j])); };
+        auto src = [&](int j) -> T {
+            return make_float2(v0 ? ldm<BarT>(&f0[j]) : 0.f, v1 ? ldm<BarT>(&f1[j]) : 0.f);
+        };
         auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
         Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst, bar);
         bar.sync();
@@ -182,8 +193,8 @@ __device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsign
             for (int k = t; k <= N / 2; k += NT) {
                 const float2 zk = sm[sidx<C>(k, q)];
                 const float2 zn = sm[sidx<C>(k == 0 ? 0 : N - k, q)];
-                A[k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-                B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
+                if (v0) A[k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                if (v1) B[k] = make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x));
             }
         }
     } else {
@@ -215,8 +226,8 @@ __device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsign
                 u = make_float2(s.x, s.y);
                 v = make_float2(s.z, s.w);
             } else {
-                u = A[k];
-                v = B[k];
+                u = v0 ? A[k] : make_float2(0.f, 0.f);
+                v = v1 ? B[k] : make_float2(0.f, 0.f);
             }
             if (j <= N / 2) return make_float2(u.x - v.y, u.y + v.x);
             return make_float2(u.x + v.y, v.x - u.y);
@@ -224,17 +235,20 @@ __device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsign
         const long long b0 = r0 * N, b1 = b0 + N;
         auto dst = [&](int j, const T& v) {
             if constexpr (OP == XR_INV_REAL) {
-                rout[b0 + j] = v.x;
-                rout[b1 + j] = v.y;
+                if (v0) rout[b0 + j] = v.x;
+                if (v1) rout[b1 + j] = v.y;
             } else {
                 static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
-                float4 p0 = psi[b0 + j], p1 = psi[b1 + j];
-                if (use_jet) {
-                    restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
-                    restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
+                if (v0) {
+                    float4 p0 = psi[b0 + j];
+                    if (use_jet) restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
+                    psi[b0 + j] = gauge4(p0, v.x);
                 }
-                psi[b0 + j] = gauge4(p0, v.x);
-                psi[b1 + j] = gauge4(p1, v.y);
+                if (v1) {
+                    float4 p1 = psi[b1 + j];
+                    if (use_jet) restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
+                    psi[b1 + j] = gauge4(p1, v.y);
+                }
             }
         };
         // k-major: the staging aliases the tile, so the first gather must
@@ -428,8 +442,13 @@ __device__ __forceinline__ void yzpass_body(const YZArgs& a, const Blk& bk, unsi
     const float2* tw = a.g.tw[a.axis];
     T x[Plan<N>::EMAX];
 
-    auto gsrc = [&](int j) -> T { return data[base + j * stride + q]; };
-    auto gdst = [&](int j, const T& v) { data[base + j * stride + q] = v; };
+    // columns past the row's end (a row length that is not a multiple of
+    // C) read zeros and store nothing
+    const bool valid = x0 + q < rl;
+    auto gsrc = [&](int j) -> T { return valid ? data[base + j * stride + q] : T{}; };
+    auto gdst = [&](int j, const T& v) {
+        if (valid) data[base + j * stride + q] = v;
+    };
 
     if constexpr (OP == YZ_FWD) {
         Plan<N>::template run<C, -1, false>(x, t, q, sm, tw, gsrc, gdst, bar);

@@ -1,6 +1,7 @@
 // Instantiations and launchers of the FFT pass kernels for every supported
-// pencil length (2^a 3^b, 8 <= n <= 512), and the dispatch over the tile
-// shape (pencil groups per CTA) chosen by the caller.
+// pencil length (2^a 3^b with 8 <= n <= 512, and 20, 40, 50, 56, 80, 100,
+// 112, 160, 200), and the dispatch over the tile shape (pencil groups per
+// CTA) chosen by the caller.
 #include "k_fftpass_impl.cuh"
 
 namespace isf {
@@ -9,6 +10,7 @@ bool supported_len(int n) {
     switch (n) {
         case 8: case 12: case 16: case 24: case 32: case 48: case 64:
         case 96: case 128: case 192: case 256: case 384: case 512:
+        case 20: case 40: case 50: case 56: case 80: case 100: case 112: case 160: case 200:
             return true;
         default:
             return false;
@@ -24,7 +26,7 @@ ISF_GROUPED_SIZES(ISF_EXT4)
 #undef ISF_EXT4
 
 bool grouped_tile_ok(int n, int groups) {
-    return groups <= 1 || ((groups == 2 || groups == 4) && n <= kMaxGroupedN && supported_len(n));
+    return groups <= 1 || ((groups == 2 || groups == 4) && grouped_size(n));
 }
 
 #define ISF_SIZE_SWITCH(n, MACRO)                  \
@@ -42,12 +44,21 @@ bool grouped_tile_ok(int n, int groups) {
         case 256: MACRO(256);                      \
         case 384: MACRO(384);                      \
         case 512: MACRO(512);                      \
+        case 20: MACRO(20);                        \
+        case 40: MACRO(40);                        \
+        case 50: MACRO(50);                        \
+        case 56: MACRO(56);                        \
+        case 80: MACRO(80);                        \
+        case 100: MACRO(100);                      \
+        case 112: MACRO(112);                      \
+        case 160: MACRO(160);                      \
+        case 200: MACRO(200);                      \
         default: return cudaErrorInvalidValue;     \
     }
 
 template <int N, int OP>
 static cudaError_t launch_x_n(const XArgs& a, cudaStream_t s) {
-    if constexpr (N <= kMaxGroupedN && grouped_x_op(OP)) {
+    if constexpr (grouped_size(N) && grouped_x_op(OP)) {
         if (a.groups == 2) return launch_x_ng<N, OP, 2>(a, s);
         if (a.groups == 4) return launch_x_ng<N, OP, 4>(a, s);
     }
@@ -79,7 +90,7 @@ static cudaError_t launch_xr_n(const XArgs& a, cudaStream_t s) {
         if (a.groups > 1) return cudaErrorInvalidValue;
         return launch_xr_ng<N, OP, 1, true>(a, s);
     }
-    if constexpr (N <= kMaxGroupedN && grouped_xr_op(OP)) {
+    if constexpr (grouped_size(N) && grouped_xr_op(OP)) {
         if (a.groups == 2) return launch_xr_ng<N, OP, 2>(a, s);
         if (a.groups == 4) return launch_xr_ng<N, OP, 4>(a, s);
     }
@@ -106,7 +117,7 @@ cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s) {
 template <int N, class T, int OP>
 static cudaError_t launch_yz_n(const YZArgs& a, cudaStream_t s) {
     constexpr bool psi = sizeof(T) == sizeof(float4);
-    if constexpr (N <= kMaxGroupedN && grouped_yz_op(OP, psi)) {
+    if constexpr (grouped_size(N) && grouped_yz_op(OP, psi)) {
         if (a.groups == 2) return launch_yz_ng<N, T, OP, 2>(a, s);
         if (a.groups == 4) return launch_yz_ng<N, T, OP, 4>(a, s);
     }

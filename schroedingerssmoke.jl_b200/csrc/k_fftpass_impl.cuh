@@ -12,6 +12,9 @@ namespace isf {
 // pencil lengths that have grouped-tile (G = 2, 4) instantiations
 constexpr int kMaxGroupedN = 128;
 #define ISF_GROUPED_SIZES(M) M(8) M(12) M(16) M(24) M(32) M(48) M(64) M(96) M(128)
+constexpr bool grouped_size(int n) {
+    return n == 8 || n == 12 || n == 16 || n == 24 || n == 32 || n == 48 || n == 64 || n == 96 || n == 128;
+}
 
 // Kernels needing more than 48 KB of dynamic shared memory must opt in once
 // per device.
@@ -35,10 +38,11 @@ cudaError_t launch_x_ng(const XArgs& a, cudaStream_t s) {
     using Sh = XShape<N, OP, G>;
     static std::atomic<unsigned long long> done{0};
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    if (rows % (Sh::C * G) != 0) return cudaErrorInvalidValue;
+    // grouped tiles need whole tiles; single groups guard a partial last one
+    if (G > 1 && rows % (Sh::C * G) != 0) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem(k_xpass<N, OP, G>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
-    const dim3 grid((unsigned)(rows / (Sh::C * G)), batch_dim(a.nsim));
+    const dim3 grid((unsigned)((rows + Sh::C * G - 1) / (Sh::C * G)), batch_dim(a.nsim));
     return launch_pdl(k_xpass<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
@@ -47,10 +51,10 @@ cudaError_t launch_xr_ng(const XArgs& a, cudaStream_t s) {
     using Sh = XRShape<N, G, KM>;
     static std::atomic<unsigned long long> done{0};
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    if (rows % (2 * Sh::C * G) != 0) return cudaErrorInvalidValue;
+    if ((G > 1 || KM) && rows % (2 * Sh::C * G) != 0) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem(k_xreal<N, OP, G, KM>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
-    const dim3 grid((unsigned)(rows / (2 * Sh::C * G)), batch_dim(a.nsim));
+    const dim3 grid((unsigned)((rows + 2 * Sh::C * G - 1) / (2 * Sh::C * G)), batch_dim(a.nsim));
     return launch_pdl(k_xreal<N, OP, G, KM>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
@@ -59,10 +63,10 @@ cudaError_t launch_yz_ng(const YZArgs& a, cudaStream_t s) {
     using Sh = YZShape<N, T, OP, G>;
     static std::atomic<unsigned long long> done{0};
     const int other = (a.axis == 1) ? a.g.n[2] : a.g.n[1];
-    if (other % G != 0 || a.row % Sh::C != 0) return cudaErrorInvalidValue;
+    if (other % G != 0 || (G > 1 && a.row % Sh::C != 0)) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem(k_yzpass<N, T, OP, G>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
-    const dim3 grid((unsigned)(a.row / Sh::C), (unsigned)(other / G), batch_dim(a.nsim));
+    const dim3 grid((unsigned)((a.row + Sh::C - 1) / Sh::C), (unsigned)(other / G), batch_dim(a.nsim));
     return launch_pdl(k_yzpass<N, T, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 

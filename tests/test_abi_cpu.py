@@ -57,7 +57,7 @@ def test_invalid_sizes_rejected_before_touching_cuda(isfpkg):
     import importlib
     _lib = importlib.import_module(isfpkg.__name__ + "._lib")
     L = _lib.load()
-    for dims in ((20, 8, 8), (8, 8, 8), (16, 8, 6), (1024, 8, 8)):
+    for dims in ((22, 8, 8), (14, 8, 8), (16, 8, 6), (16, 9, 8), (1024, 8, 8)):
         p = _lib.IsfParams()
         p.grid_res[:] = list(dims)
         p.physical_size[:] = [1, 1, 1]

@@ -15,6 +15,10 @@ GRIDS = [
     ((3, 2, 2), (48, 32, 32)),
     ((6, 3, 3), (96, 48, 48)),
     ((2, 1, 1), (32, 12, 24)),
+    # lengths with factors 5 and 7; rows and x extents that are not whole tiles
+    ((4, 2, 2), (80, 40, 40)),
+    ((4, 2, 2), (100, 50, 50)),
+    ((2, 1, 1), (56, 20, 28)),
 ]
 HBAR = float(np.float32(0.1))
 DT = float(np.float32(1 / 48))
@@ -29,7 +33,8 @@ def host(t):
 
 
 @pytest.mark.parametrize("dims", [(16, 8, 8), (32, 12, 24), (48, 32, 32), (96, 48, 48), (256, 128, 128),
-                                  (512, 16, 8), (384, 8, 16), (192, 64, 8)])
+                                  (512, 16, 8), (384, 8, 16), (192, 64, 8), (80, 40, 40), (100, 50, 50),
+                                  (56, 112, 20), (200, 50, 160)])
 def test_fft3_matches_numpy(isfpkg, dims):
     isf = isfpkg.ISF((1, 1, 1), dims, HBAR, DT)
     rng = np.random.default_rng(1)
