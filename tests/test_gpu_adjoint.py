@@ -307,7 +307,15 @@ def test_adj_gradient_jet_64x32x32_50_steps(isfpkg, oracle_mod, cfgs):
     (psi1 = 1, psi2 = 0.01) the loss is stationary: a perturbation changes the
     velocity to first order only by an exact one-form, which the projection
     removes, so positions move as h^2 and every directional derivative in psi0
-    vanishes (as do those in kvec and omega, a gauge).  Every one of the 8
+    vanishes (as do those in kvec and omega, a gauge).
+
+    Over 50 steps the FP32 and FP64 trajectories of a particle whose RK
+    sample points pass within rounding distance of a cell face can use
+    different cells, where the unnormalised interpolation's derivative
+    differs (about 0.2 % of the gradient with every particle kept).  As in
+    the forward parity tests, the particles whose FP64 sample points came
+    within 1e-4 cells of a face are left out (dead from the start, so
+    neither the GPU loss nor the oracle's includes them).  Every one of the 8
     psi0 directions and 2 particle directions drawn is checked, each with a
     crossing-free step from fd_without_crossing, within 1e-3."""
     c = cfgs.CONFIGS["C1"]
@@ -322,18 +330,26 @@ def test_adj_gradient_jet_64x32x32_50_steps(isfpkg, oracle_mod, cfgs):
     p0 = f32(rng.uniform(0.1, 0.9, (P, 3)) * np.asarray(Lc))
     psi0 = f32(smooth_psi(dims, 5))
 
-    def forward(psi, x):
+    def forward(psi, x, margin=None):
         psi, x = psi.copy(), x.copy()
         for _ in range(I):
             orc.restrict_velocity(psi, kvec, 0.0, *nozzle, phase_mode=1)
             orc.pressure_project(psi)
         for n in range(1, T + 1):
             tn = float(np.float32(n) * np.float32(c["dt"]))
+            m = np.zeros(len(x)) if margin is not None else None
             orc.step(psi, x, dict(kvec=kvec, omega_t=omega * tn, cen=noz["cen"], len=noz["len"], rad=noz["rad"],
-                                  emit_count=0, counter=n, phase_mode=1))
+                                  emit_count=0, counter=n, phase_mode=1), margin=m)
+            if margin is not None:
+                np.minimum(margin, m, out=margin)
         return x
 
-    tgt = f32(forward(psi0, p0) + rng.normal(0, 0.1, p0.shape))
+    margin = np.full(P, 1e30)
+    xT = forward(psi0, p0, margin)
+    near = margin <= 1e-4
+    assert near.mean() < 0.2, near.mean()
+    p0[near] = -1.0
+    tgt = f32(xT + rng.normal(0, 0.1, p0.shape))
 
     def Lf(dpsi=0.0, dp=0.0):
         x = forward(psi0 + dpsi, p0 + dp)

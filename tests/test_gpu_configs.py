@@ -180,7 +180,7 @@ def test_jet_128x64x64_200_steps(isfpkg, oracle_mod, cfgs):
                    phase_mode=isfpkg.PHASE_DOT)
         if it > horizon:
             isf.sync()
-            mpsi, mp = host(psi), host(parts)[sub]
+            mpsi, mp = host(psi), np.ascontiguousarray(host(parts)[sub])
         isfpkg.step(isf, psi, parts, jet)
         m = np.zeros(n)
         o64.step(psi64, p64, jet, margin=m)
