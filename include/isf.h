@@ -375,7 +375,8 @@ ISF_API int isf_batch_sync(isf_batch* b);
  * naming the pass; the state is then partly stepped.  ISF_PERSIST_STALL adds
  * a wait on a flag that nothing sets to every dependent pass, so the timeout
  * path can be exercised without a fault.  Needs every class to have nx in
- * {16,32,48,64,96,128} and ny = nz in {32,48,64,96} (ISF_ERR_INVALID
+ * {16,32,48,64,96,128} and ny = nz in {32,48,64,96}, and at most 255 passes
+ * per ensemble step in all (about a dozen classes; ISF_ERR_INVALID
  * otherwise).  Mode 0 returns to the per-step graph.  Reference: the
  * ensemble is new; each simulation's step is examples/benchmark.jl:46-65. */
 enum { ISF_PERSIST_ON = 1, ISF_PERSIST_STALL = 2 };

@@ -498,7 +498,7 @@ bool class_chain(const isf_batch* b, const BatchClass& c, int ci, std::vector<PP
     v.st.sharp = 1;
     out.push_back(v);
     if (c.key.nslots > 0) {
-        PPhase a = new_phase(c, ci, PK_ADVECT, 0, up(c.key.nslots, kPersistThreads), ns, 1);
+        PPhase a = new_phase(c, ci, PK_ADVECT, 0, up(c.key.nslots, (long long)kPersistThreads * kAdvectSlots), ns, 1);
         a.parts = c.parts;
         a.nslots = c.key.nslots;
         a.vel = c.vel;
@@ -518,8 +518,15 @@ int build_plan(isf_batch* b, int vper_div, int blocks_per_sm_cap) {
     for (size_t ci = 0; ci < b->cls.size(); ++ci)
         if (!class_chain(b, b->cls[ci], (int)ci, chains[ci], b->persist_why))
             return bfail(b, ISF_ERR_INVALID, b->persist_why);
-    size_t maxlen = 0;
-    for (auto& ch : chains) maxlen = std::max(maxlen, ch.size());
+    size_t maxlen = 0, nslot = 0;
+    for (auto& ch : chains) {
+        maxlen = std::max(maxlen, ch.size());
+        nslot += ch.size();
+    }
+    if (nslot > (size_t)kPersistMaxSlots)
+        return bfail(b, ISF_ERR_INVALID, "persistent kernel: " + std::to_string(nslot) + " passes per step (" +
+                                             std::to_string(b->cls.size()) + " classes); at most " +
+                                             std::to_string(kPersistMaxSlots));
     std::vector<std::vector<int>> slot_of(chains.size());
     std::vector<PPhase> ph;
     for (size_t j = 0; j < maxlen; ++j)
@@ -860,6 +867,11 @@ int isf_batch_create(const isf_sim_desc* sims, int32_t nsims, int32_t device, in
         b->persist_ok = true;
         for (size_t ci = 0; ci < b->cls.size() && b->persist_ok; ++ci)
             b->persist_ok = class_chain(b, b->cls[ci], (int)ci, probe, pwhy);
+        if (b->persist_ok && probe.size() > (size_t)kPersistMaxSlots) {
+            b->persist_ok = false;
+            pwhy = "the persistent kernel holds at most " + std::to_string(kPersistMaxSlots) +
+                   " passes per step; these classes have " + std::to_string(probe.size());
+        }
         b->persist_why = pwhy;
     }
     if (b->persist_ok && e == cudaSuccess) {

@@ -138,6 +138,38 @@ __device__ __forceinline__ void dft7(T* x) {
     dft_odd<7, S>(x, c, sn);
 }
 
+// 16 = 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2;
+//   X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 w4^(n1 k1) x[4 n1 + n2]
+template <int S, class T>
+__device__ __forceinline__ void dft16(T* x) {
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<S>(x[n2], x[4 + n2], x[8 + n2], x[12 + n2]);
+    // twiddles w16^(n2 k1) on y[n2][k1] = x[4 k1 + n2], w16 = exp(S 2 pi i / 16)
+    const float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+    const float Sf = S < 0 ? -1.f : 1.f;
+    x[5] = cmul(x[5], make_float2(c1, Sf * s1));    // n2 = 1, k1 = 1: w^1
+    x[9] = cmul(x[9], make_float2(h, Sf * h));      // n2 = 1, k1 = 2: w^2
+    x[13] = cmul(x[13], make_float2(s1, Sf * c1));  // n2 = 1, k1 = 3: w^3
+    x[6] = cmul(x[6], make_float2(h, Sf * h));      // n2 = 2, k1 = 1: w^2
+    x[10] = mul_si<S>(x[10]);                       // n2 = 2, k1 = 2: w^4
+    x[14] = cmul(x[14], make_float2(-h, Sf * h));   // n2 = 2, k1 = 3: w^6
+    x[7] = cmul(x[7], make_float2(s1, Sf * c1));    // n2 = 3, k1 = 1: w^3
+    x[11] = cmul(x[11], make_float2(-h, Sf * h));   // n2 = 3, k1 = 2: w^6
+    x[15] = cmul(x[15], make_float2(-c1, -Sf * s1));  // n2 = 3, k1 = 3: w^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<S>(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+    // x[4 k1 + k2] holds X[k1 + 4 k2]: transpose the 4 x 4 block
+    T t;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = a + 1; b < 4; ++b) {
+            t = x[4 * a + b];
+            x[4 * a + b] = x[4 * b + a];
+            x[4 * b + a] = t;
+        }
+}
+
 template <int R, int S, class T>
 __device__ __forceinline__ void dft(T* x) {
     if constexpr (R == 2) dft2<S>(x[0], x[1]);
@@ -146,6 +178,7 @@ __device__ __forceinline__ void dft(T* x) {
     else if constexpr (R == 5) dft5<S>(x);
     else if constexpr (R == 7) dft7<S>(x);
     else if constexpr (R == 8) dft8<S>(x);
+    else if constexpr (R == 16) dft16<S>(x);
     else static_assert(R == 2, "unsupported radix");
 }
 
@@ -271,9 +304,10 @@ constexpr int isf_emax(int N, int NT, std::initializer_list<int> rs) {
 // inverse of run_spectral).
 template <int N>
 struct Plan;
-#define ISF_PLAN(NN, R0, FWD, REV)                                                                          \
+#define ISF_PLAN(NN, R0, FWD, REV) ISF_PLAN_NAMED(Plan, NN, R0, FWD, REV)
+#define ISF_PLAN_NAMED(NAME, NN, R0, FWD, REV)                                                              \
     template <>                                                                                             \
-    struct Plan<NN> {                                                                                       \
+    struct NAME<NN> {                                                                                       \
         static constexpr int first = R0;                                                                    \
         static constexpr int NT = NN / R0;                                                                  \
         static constexpr int EMAX = isf_emax(NN, NN / R0, {ISF_UNPAREN FWD});                              \
@@ -330,5 +364,20 @@ ISF_PLAN(112, 4, (4, 4, 7), (7, 4, 4))
 ISF_PLAN(160, 8, (8, 4, 5), (5, 4, 8))
 ISF_PLAN(200, 8, (8, 5, 5), (5, 5, 8))
 #undef ISF_PLAN
+
+// Plans of the (y, z) plane Poisson solver: Plan<N>, except N = 128 in two
+// stages (16, 8), one shared-memory exchange per transform instead of two.
+// The plane kernel keeps its pencils in shared memory, so its time follows
+// the exchanges; the radix-16 butterfly's 16 complex registers per thread
+// fit its float2 data (the psi passes keep Plan<128>).
+#ifndef ISF_PLANE128_RADIX16
+#define ISF_PLANE128_RADIX16 1
+#endif
+template <int N>
+struct PlanPlane : Plan<N> {};
+#if ISF_PLANE128_RADIX16
+ISF_PLAN_NAMED(PlanPlane, 128, 16, (16, 8), (8, 16))
+#endif
+#undef ISF_PLAN_NAMED
 
 }  // namespace isf

@@ -282,11 +282,17 @@ struct PlaneArgs {
 #ifndef ISF_PLANE_MAX_THREADS
 #define ISF_PLANE_MAX_THREADS 1024
 #endif
+// the 128 x 128 plane's radix-16 pencils hold twice the registers per thread
+#ifndef ISF_PLANE128_MAX_THREADS
+#define ISF_PLANE128_MAX_THREADS 512
+#endif
+template <int N>
+constexpr int plane_max_threads() { return N == 128 ? ISF_PLANE128_MAX_THREADS : ISF_PLANE_MAX_THREADS; }
 
-template <int N, int MAXT = ISF_PLANE_MAX_THREADS>
+template <int N, int MAXT = plane_max_threads<N>()>
 struct PlaneShape {
     static constexpr int C = 16;
-    static constexpr int NT = Plan<N>::NT;
+    static constexpr int NT = PlanPlane<N>::NT;
     static constexpr int GT = C * NT;  // threads of one pencil group
     static constexpr int GMAX = MAXT / GT > 0 ? MAXT / GT : 1;
     static constexpr int GROUPS = GMAX < (N / C) ? GMAX : (N / C);
@@ -305,7 +311,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs& a, const Blk& bk, un
     float2* tile = plane + N * N + grp * (N * C);
     const int kx = bk.x;
     float2* __restrict__ Fp = a.F + bk.y * a.bs_F + (long long)kx * N * N;
-    float2 x[Plan<N>::EMAX];
+    float2 x[PlanPlane<N>::EMAX];
     const float2 zero = make_float2(0.f, 0.f);
     // y transforms: pencil = row z of the plane, lanes along y.  The forward
     // one reads its rows straight from HBM into registers and leaves them in
@@ -328,7 +334,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs& a, const Blk& bk, un
                 else
                     Fp[z * N + j] = v;
             };
-            Plan<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst, bar);
+            PlanPlane<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst, bar);
             bar.sync();
         }
     };
@@ -356,7 +362,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs& a, const Blk& bk, un
                 const float f = (zero_line && j == 0) ? 0.f : (float)(sc * __drcp_rn(dxo + __ldg(&s2z[j])));
                 return cscale(v, f);
             };
-            Plan<N>::template run_spectral<C>(x, t, q, tile, a.g.tw[2], src, fmul, dst, bar);
+            PlanPlane<N>::template run_spectral<C>(x, t, q, tile, a.g.tw[2], src, fmul, dst, bar);
             bar.sync();
         }
     }

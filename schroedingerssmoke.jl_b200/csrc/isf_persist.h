@@ -81,6 +81,10 @@ struct PPlan {
 };
 
 constexpr int kPersistThreads = 256;
+// slots (passes of all classes in one step) the kernel's shared slot table holds
+constexpr int kPersistMaxSlots = 255;
+// slots an advection thread steps per work item
+constexpr int kAdvectSlots = 4;
 // x pencil lengths and (y, z) plane sizes the persistent kernel is built for
 bool persist_len_ok(int n);
 bool persist_plane_ok(int n);

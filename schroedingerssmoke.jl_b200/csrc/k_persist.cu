@@ -40,9 +40,9 @@ __device__ __forceinline__ void with_plane(int n, const F& f) {
 template <int N>
 using PShape = PlaneShape<N, kPersistThreads>;
 
-__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 __device__ __forceinline__ int ld_relaxed(const int* p) {
@@ -51,11 +51,12 @@ __device__ __forceinline__ int ld_relaxed(const int* p) {
     return v;
 }
 
-// Poll *p until it reaches need, at most limit times; false if the limit ran
-// out or another block reported an error.
+// Poll *p (acquire: what the counted items wrote is visible after it) until
+// it reaches need, at most limit times; false if the limit ran out or
+// another block reported an error.
 __device__ bool bounded_wait(const unsigned* p, unsigned need, long long limit, const int* status) {
     for (long long k = 0;; ++k) {
-        if (ld_relaxed(p) >= need) return true;
+        if (ld_acquire(p) >= need) return true;
         if (ld_relaxed(status) != 0 || k >= limit) return false;
         __nanosleep(k < 64 ? 32 : 256);
     }
@@ -138,12 +139,14 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
             break;
         }
         case PK_ADVECT: {
-            const long long k = (long long)bk.x * ph.vblk + vt;
+            // kAdvectSlots slots per thread: slot bk.x * vblk * kAdvectSlots + j vblk + vt
             unsigned clamps = 0, live = 0;
-            if (k < ph.nslots) {
-                const AdvConst kc = adv_const(ph.g, ph.vel + bk.y * ph.bs_vel);
-                const float dt = ph.g.dt, s6 = ph.g.dt / 6.0f;
-                float* parts = ph.parts + bk.y * 3 * ph.nslots;
+            const AdvConst kc = adv_const(ph.g, ph.vel + bk.y * ph.bs_vel);
+            const float dt = ph.g.dt, s6 = ph.g.dt / 6.0f;
+            float* parts = ph.parts + bk.y * 3 * ph.nslots;
+            for (int j = 0; j < kAdvectSlots; ++j) {
+                const long long k = ((long long)bk.x * kAdvectSlots + j) * ph.vblk + vt;
+                if (k >= ph.nslots) break;
                 if (ph.normw) {
                     if (ph.pow2)
                         advect_slot<true, true, NamedBar>(kc, parts, (int)k, dt, s6, clamps, live, nullptr);
@@ -179,22 +182,31 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
 __global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int s_item, s_go;
+    __shared__ int s_start[kPersistMaxSlots + 1];  // the slot table, searched per item
+    for (int i = threadIdx.x; i <= P.nslot; i += blockDim.x) s_start[i] = P.slot_start[i];
     const int total = P.items_per_step * P.nsteps;
+    // thread 0 claims the block's next item while the block works on the
+    // current one (the lowest unfinished item always belongs to a block
+    // that runs it or starts it next, so the waits still resolve)
+    int next = threadIdx.x == 0 ? (int)atomicAdd(&P.ctl[0], 1u) : 0;
     for (;;) {
         if (threadIdx.x == 0) {
-            int it = -1;
-            if (ld_relaxed(&P.status[0]) == 0) {
-                it = (int)atomicAdd(&P.ctl[0], 1u);
-                if (it >= total) it = -1;
-            }
+            int it = next;
+            if (it >= total || ld_relaxed(&P.status[0]) != 0) it = -1;
+            if (it >= 0) next = (int)atomicAdd(&P.ctl[0], 1u);
             s_item = it;
         }
         __syncthreads();
         const int it = s_item;
         if (it < 0) break;
         const int step = it / P.items_per_step, r = it - step * P.items_per_step;
-        int slot = 0;
-        while (P.slot_start[slot + 1] <= r) ++slot;
+        int lo = 0, hi = P.nslot - 1;  // the slot with s_start[slot] <= r < s_start[slot + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_start[mid] <= r) lo = mid;
+            else hi = mid - 1;
+        }
+        const int slot = lo;
         const PPhase& ph = P.ph[slot];
         if (threadIdx.x == 0) {
             bool ok = true;
@@ -209,13 +221,12 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
             if (ok && P.stall && (ph.dep >= 0 || (step > 0 && ph.dep_prev >= 0)))
                 ok = bounded_wait(reinterpret_cast<const unsigned*>(&P.status[3]), 1u, P.spin_limit, P.status);
             if (!ok) report(P, slot, step);
-            __threadfence();  // acquire: this item's reads see the predecessor's writes
             s_go = ok ? 1 : 0;
         }
         __syncthreads();
         if (!s_go) break;
         const int v = threadIdx.x / ph.vblk;
-        const int tile = (r - P.slot_start[slot]) * ph.vper + v;
+        const int tile = (r - s_start[slot]) * ph.vper + v;
         if (v < ph.vper && tile < ph.tiles)
             run_tile(P, ph, tile, step, threadIdx.x - v * ph.vblk, smraw + v * ph.smem_v, NamedBar{1 + v, ph.vblk});
         __syncthreads();  // every virtual CTA of the item is done

@@ -162,7 +162,7 @@ def test_batch_against_fp64_oracle(isfpkg, oracle_mod, cfgs):
 def test_batch_errors(isfpkg, cfgs):
     sims, psi0, parts0 = small_ensemble(cfgs)
     bad = [dict(sims[0]), dict(sims[1])]
-    bad[1]["dims"] = (24, 32, 32)
+    bad[1]["dims"] = (22, 32, 32)
     with pytest.raises(isfpkg.ISFError, match="simulation 1"):
         isfpkg.ISFBatch(bad)
     bad = [dict(sims[0])]

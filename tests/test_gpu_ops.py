@@ -18,7 +18,9 @@ GRIDS = [
     # lengths with factors 5 and 7; rows and x extents that are not whole tiles
     ((4, 2, 2), (80, 40, 40)),
     ((4, 2, 2), (100, 50, 50)),
-    ((2, 1, 1), (56, 20, 28)),
+    ((2, 1, 1), (56, 20, 40)),
+    # the 128 x 128 plane solver (radix 16 x 8)
+    ((1, 4, 4), (32, 128, 128)),
 ]
 HBAR = float(np.float32(0.1))
 DT = float(np.float32(1 / 48))
@@ -252,9 +254,9 @@ def test_step_sequences(isfpkg, oracle_mod, cfgs, L, dims):
 
 def test_invalid_arguments(isfpkg):
     with pytest.raises(isfpkg.ISFError):
-        isfpkg.ISF((1, 1, 1), (20, 8, 8), HBAR, DT)  # 20 is not 2^a 3^b
+        isfpkg.ISF((1, 1, 1), (22, 8, 8), HBAR, DT)  # 22 = 2 x 11: no radix plan
     with pytest.raises(isfpkg.ISFError):
-        isfpkg.ISF((1, 1, 1), (8, 8, 8), HBAR, DT)   # nx < 16
+        isfpkg.ISF((1, 1, 1), (16, 8, 28), HBAR, DT)  # 28 is not one of the plans' lengths
     isf = isfpkg.ISF((1, 1, 1), (16, 8, 8), HBAR, DT)
     bad = torch.zeros((8, 8, 8, 4), device="cuda")
     with pytest.raises(isfpkg.ISFError):
