@@ -20,7 +20,7 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NO_TMA, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
                    PHASE_REFERENCE_SUM, IsfParams, IsfStepArgs, ISFError, check, f3)
 
 __all__ = [
@@ -152,7 +152,8 @@ class ISF:
         out = (C.c_uint64 * 16)()
         check(self.L.isf_counters(self.h, out, 16, int(reset)), self.h)
         return {"clamp_events": int(out[0]), "live": int(out[1]), "check_failures": int(out[2]),
-                "first_bad_index": int(out[3]), "first_bad_context": [int(v) for v in out[4:12]]}
+                "first_bad_index": int(out[3]), "first_bad_context": [int(v) for v in out[4:12]],
+                "wait_timeouts": int(out[14]), "nonfinite": int(out[15])}
 
     def counters_async(self, out: torch.Tensor, reset: bool = False):
         """Queue a copy of the advection counters [clamp events, live] into

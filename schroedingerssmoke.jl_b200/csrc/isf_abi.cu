@@ -17,6 +17,10 @@
 
 namespace isf {
 
+// tests of one mbarrier wait of the TMA-staged pass before it gives up (a
+// tile arrives within microseconds; this is about half a second)
+constexpr long long kTmaWaitLimit = 1LL << 22;
+
 int half_spectrum_row(int nx) { return ((nx / 2 + 1 + 15) / 16) * 16; }
 
 size_t table_bytes(const int n[3]) {
@@ -120,7 +124,7 @@ bool check_params(const isf_params* p, std::string& why) {
         why = "hbar and dt must be finite, dt > 0";
         return false;
     }
-    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN)) {
+    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN | ISF_FLAG_NO_TMA)) {
         why = "unknown flags";
         return false;
     }
@@ -231,7 +235,18 @@ int run_schroedinger(isf_handle* h, float* psi, bool norm) {
     xa.psi = reinterpret_cast<float4*>(psi);
     ISF_LAUNCH(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
     ISF_LAUNCH(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
-    ISF_LAUNCH(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");
+    // the z pass with TMA-staged pencils where it is built for the length
+    bool tma = !(h->flags & ISF_FLAG_NO_TMA) && zmask_tma_len(h->g.n[2]) && h->g.n[0] % 8 == 0;
+    if (tma && h->zmap_psi != psi) {
+        h->zmap_ok = encode_psi_zmap(&h->zmap, psi, h->g);
+        h->zmap_psi = psi;
+    }
+    tma = tma && h->zmap_ok;
+    if (tma)
+        ISF_LAUNCH(h, launch_zmask_tma(h->zmap, yzargs(h, psi, 2), kTmaWaitLimit, h->counters + 14, h->stream),
+                   "schroedinger z mask");
+    else
+        ISF_LAUNCH(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");
     ISF_LAUNCH(h, launch_yzpass_psi(YZ_INV, yzargs(h, psi, 1), h->stream), "schroedinger y inv");
     ISF_LAUNCH(h, launch_xpass(norm ? X_PSI_INV_NORM : X_PSI_INV, xa, h->stream), "schroedinger x inv");
     return ISF_OK;

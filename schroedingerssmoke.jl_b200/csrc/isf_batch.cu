@@ -116,7 +116,7 @@ struct isf_batch {
     int* d_status = nullptr;
     long long spin_limit = 1LL << 22;
     int pgrid = 0, psmem = 0;
-    int pvper_div = 1;             // tuned: virtual CTAs per item = max / pvper_div
+    int preps = 1;                 // tuned: tiles per virtual CTA and item
     std::map<int, cudaGraphExec_t> pgraphs;
 };
 
@@ -512,8 +512,9 @@ bool class_chain(const isf_batch* b, const BatchClass& c, int ci, std::vector<PP
 
 // The slot table: the classes' chains interleaved pass by pass, each phase
 // waiting for its predecessor (the class's last phase of the previous step
-// for the first one); `vper_div` divides the virtual CTAs per item.
-int build_plan(isf_batch* b, int vper_div, int blocks_per_sm_cap) {
+// for the first one); an item is as many virtual CTAs as fit a block, each
+// running `reps` tiles.
+int build_plan(isf_batch* b, int reps, int blocks_per_sm_cap) {
     std::vector<std::vector<PPhase>> chains(b->cls.size());
     for (size_t ci = 0; ci < b->cls.size(); ++ci)
         if (!class_chain(b, b->cls[ci], (int)ci, chains[ci], b->persist_why))
@@ -550,9 +551,9 @@ int build_plan(isf_batch* b, int vper_div, int blocks_per_sm_cap) {
             return bfail(b, ISF_ERR_INVALID, "persistent kernel: pass kind " + std::to_string(p.kind) + " of length " +
                                                  std::to_string(p.len) + " has no virtual CTA shape");
         p.smem_v = persist_smem(p.kind, p.len);
-        const int vmax = std::max(1, kPersistThreads / p.vblk);
-        p.vper = std::max(1, vmax / vper_div);
-        p.items = (p.tiles + p.vper - 1) / p.vper;
+        p.vper = std::max(1, kPersistThreads / p.vblk);
+        p.reps = p.kind == PK_PROLOGUE ? 1 : reps;
+        p.items = (p.tiles + p.vper * p.reps - 1) / (p.vper * p.reps);
         smem = std::max(smem, p.vper * p.smem_v);
         start.push_back(start.back() + p.items);
     }
@@ -576,7 +577,7 @@ int build_plan(isf_batch* b, int vper_div, int blocks_per_sm_cap) {
     b->slot_start = start;
     b->psmem = smem;
     b->pgrid = sms * bps;
-    b->pvper_div = vper_div;
+    b->preps = reps;
     return ISF_OK;
 }
 
@@ -627,20 +628,20 @@ int ensure_done(isf_batch* b, long long nsteps) {
     return ISF_OK;
 }
 
-// The persistent kernel's tile autotuner: virtual CTAs per work item (all
-// that fit a block, or half of them) and blocks per SM (as many as fit, or
-// one), each timed over 3 steps of the zeroed state; keeps the fastest.
+// The persistent kernel's tile autotuner: tiles per virtual CTA and item
+// (1, 2 or 4) and blocks per SM (as many as fit, or one), each timed over 3
+// steps of the zeroed state; keeps the fastest.
 int tune_persist(isf_batch* b, bool tune) {
-    int best_div = 1, best_bps = 2;
+    int best_reps = 1, best_bps = 2;
     if (tune) {
         cudaEvent_t e0, e1;
         B_CUDA(b, cudaEventCreate(&e0), "persistent tuning");
         B_CUDA(b, cudaEventCreate(&e1), "persistent tuning");
         float best = 1e30f;
         int rc = ISF_OK;
-        for (int div : {1, 2}) {
+        for (int reps : {1, 2, 4}) {
             for (int bps : {2, 1}) {
-                if ((rc = build_plan(b, div, bps)) != ISF_OK) break;
+                if ((rc = build_plan(b, reps, bps)) != ISF_OK) break;
                 if ((rc = ensure_done(b, 3)) != ISF_OK) break;
                 cudaError_t e = queue_persist(b, 3, b->stream);  // warm-up
                 if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
@@ -661,7 +662,7 @@ int tune_persist(isf_batch* b, bool tune) {
                 }
                 if (ms < best * 0.97f) {
                     best = ms;
-                    best_div = div;
+                    best_reps = reps;
                     best_bps = bps;
                 }
             }
@@ -671,7 +672,7 @@ int tune_persist(isf_batch* b, bool tune) {
         cudaEventDestroy(e1);
         if (rc != ISF_OK) return rc;
     }
-    if (int rc = build_plan(b, best_div, best_bps)) return rc;
+    if (int rc = build_plan(b, best_reps, best_bps)) return rc;
     return ensure_done(b, 1);
 }
 

@@ -320,13 +320,15 @@ struct Plan;
             pipeline<NN, NN / R0, C, S, T, Dst, B, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, dst, bar);          \
         }                                                                                                   \
         /* forward transform, mul(j, v) on every output j in registers, inverse transform */               \
-        template <int C, class T, class Src, class Mul, class Dst, class B = CtaBar>                        \
+        /* (SYNC: barrier after the first gather, when src reads the tile)  */                             \
+        template <int C, bool SYNC = false, class T, class Src, class Mul, class Dst, class B = CtaBar>     \
         static __device__ __forceinline__ void run_spectral(T* x, int t, int q, T* sm,                      \
                                                             const float2* __restrict__ tw, const Src& src,  \
                                                             const Mul& mul, const Dst& dst,                 \
                                                             const B& bar = B()) {                           \
             constexpr int NTh = NN / R0;                                                                    \
             gather<NN, NTh, R0>(x, t, src);                                                                 \
+            if constexpr (SYNC) bar.sync();                                                                 \
             pipeline_keep<NN, NTh, C, -1, T, B, 1, ISF_UNPAREN FWD>(x, t, q, sm, tw, bar);                  \
             constexpr int RL = First<ISF_UNPAREN REV>::value, PL = NN / RL;                                 \
             constexpr int NBT = Stage<NN, NTh, RL>::NBT;                                                    \

@@ -56,6 +56,10 @@ struct isf_handle {
     const float* order_parts = nullptr;  // the slot array it was made for
     isf::OrderBufs ord = {};
     long long ord_cap = 0;               // slots the rank / order buffers hold
+    // the tensor map of the TMA-staged z pass, for the psi it was encoded for
+    isf::CUtensorMapStorage zmap = {};
+    const float* zmap_psi = nullptr;
+    bool zmap_ok = false;
 };
 
 namespace isf_int {

@@ -54,6 +54,17 @@ cudaError_t launch_yzpass_c(int op, const YZArgs& a, cudaStream_t s);
 bool plane_supported(const int n[3]);
 cudaError_t launch_poisson_plane(const Grid& g, float2* F, long long bs_F, int nsim, cudaStream_t s);
 
+// The Schroedinger z pass with TMA-staged pencils (k_ztma.cu): the storage
+// of a CUtensorMap (128 bytes) describing psi, encoded for psi's address;
+// err counts mbarrier waits that ran out (the CTA then returns)
+struct alignas(64) CUtensorMapStorage {
+    unsigned long long q[16];
+};
+bool zmask_tma_len(int n);
+bool encode_psi_zmap(CUtensorMapStorage* out, const float* psi, const Grid& g);
+cudaError_t launch_zmask_tma(const CUtensorMapStorage& map, const YZArgs& a, long long limit, unsigned long long* err,
+                             cudaStream_t s);
+
 // z-marching stencils of the one-form (k_stencil.cu)
 enum StOp { ST_DIV = 0, ST_VEL = 1 };
 struct StencilArgs {

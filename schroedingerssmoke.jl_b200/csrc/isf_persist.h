@@ -45,7 +45,8 @@ struct PPhase {
     int kind, cls;
     int len;            // pencil length of an FFT pass
     int vblk, vper;     // threads per virtual CTA, virtual CTAs per item
-    int tiles, items;   // tiles of the pass, items = ceil(tiles / vper)
+    int reps;           // tiles a virtual CTA runs one after another in an item
+    int tiles, items;   // tiles of the pass, items = ceil(tiles / (vper reps))
     int gx, gy;         // tile t -> block (t % gx, (t / gx) % gy, t / (gx gy))
     int dep;            // slot of the same step this phase waits for (-1: none)
     int dep_prev;       // slot of the previous step it waits for (-1: none)
@@ -69,7 +70,7 @@ struct PPlan {
     const int* slot_start;   // nslot + 1: first item of each slot within a step
     int nslot, items_per_step, nsteps;
     unsigned* done;          // nsteps x nslot items finished (zeroed before the launch)
-    unsigned* ctl;           // [0] next item, [1] items finished (zeroed before the launch)
+    unsigned* ctl;           // [0] next item, [1] slots finished in the last step (zeroed before the launch)
     int* status;             // [0] error code, [1] slot, [2] step, [3] a flag nothing sets (zeroed)
     long long spin_limit;    // polls of one wait before it gives up
     int stall;               // 1: the first dependent item also waits for status[3] (a timeout by construction)

@@ -39,15 +39,23 @@ constexpr int LPT = (TILE + BX * TY - 1) / (BX * TY);           // tile loads pe
 
 }  // namespace st
 
-// shared memory of one stencil CTA
+// shared memory of one stencil CTA: the psi tiles, and for the divergence
+// the x / y one-form edges (the one-form stencil leaves them out, which
+// leaves more of the SM's shared storage to L1)
+template <int OP>
 struct StencilSmem {
     float4 tile[2][st::TH][st::TW];
     float vxs[st::BY][st::BX + 1];  // v_x at x0-1+c (c = 0..W)
     float vys[st::BY + 1][st::BX];  // v_y at y0-1+r (r = 0..H)
 };
+template <>
+struct StencilSmem<ST_VEL> {
+    float4 tile[2][st::TH][st::TW];
+};
 
 template <int OP, class B = CtaBar>
-__device__ __forceinline__ void stencil_body(const StencilArgs& a, const Blk& bk, StencilSmem& S, const B& bar = B()) {
+__device__ __forceinline__ void stencil_body(const StencilArgs& a, const Blk& bk, StencilSmem<OP>& S,
+                                             const B& bar = B()) {
     using namespace st;
     const Grid& g = a.g;
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
@@ -66,8 +74,6 @@ __device__ __forceinline__ void stencil_body(const StencilArgs& a, const Blk& bk
     for (int m = 0; m < RPT; ++m) own[m] = (tx < W) && (ty + TY * m < H);
 
     auto& tile = S.tile;
-    auto& vxs = S.vxs;
-    auto& vys = S.vys;
 
     // Each thread loads the same LPT padded-tile elements in every plane:
     // padded column c <-> x0 + c - 1 and row r <-> y0 + r - 1 (periodic), so
@@ -156,6 +162,8 @@ __device__ __forceinline__ void stencil_body(const StencilArgs& a, const Blk& bk
                 if (tsl[k] >= 0) pre[k] = tile_e(k, z2);
         }
         if constexpr (OP == ST_DIV) {
+            auto& vxs = S.vxs;
+            auto& vys = S.vys;
 #pragma unroll
             for (int m = 0; m < RPT; ++m) {
                 const int r = ty + TY * m;

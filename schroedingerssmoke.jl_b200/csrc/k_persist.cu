@@ -120,10 +120,10 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
             });
             break;
         case PK_DIV:
-            stencil_body<ST_DIV>(ph.st, bk, *reinterpret_cast<StencilSmem*>(sm), bar);
+            stencil_body<ST_DIV>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_DIV>*>(sm), bar);
             break;
         case PK_VEL:
-            stencil_body<ST_VEL>(ph.st, bk, *reinterpret_cast<StencilSmem*>(sm), bar);
+            stencil_body<ST_VEL>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
             break;
         case PK_EMIT: {
             const long long j = (long long)bk.x * ph.vblk + vt;
@@ -225,16 +225,25 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
         }
         __syncthreads();
         if (!s_go) break;
+        // the item: reps rounds of vper virtual CTAs, one tile each per round
         const int v = threadIdx.x / ph.vblk;
-        const int tile = (r - s_start[slot]) * ph.vper + v;
-        if (v < ph.vper && tile < ph.tiles)
-            run_tile(P, ph, tile, step, threadIdx.x - v * ph.vblk, smraw + v * ph.smem_v, NamedBar{1 + v, ph.vblk});
+        if (v < ph.vper) {
+            const NamedBar bar{1 + v, ph.vblk};
+            for (int rr = 0; rr < ph.reps; ++rr) {
+                const int tile = ((r - s_start[slot]) * ph.reps + rr) * ph.vper + v;
+                if (tile >= ph.tiles) break;
+                if (rr > 0) bar.sync();  // the previous tile's last reads of the shared tile are done
+                run_tile(P, ph, tile, step, threadIdx.x - v * ph.vblk, smraw + v * ph.smem_v, bar);
+            }
+        }
         __syncthreads();  // every virtual CTA of the item is done
         if (threadIdx.x == 0) {
             __threadfence();  // release: the item's writes before its count
-            atomicAdd(&P.done[step * P.nslot + slot], 1u);
-            // the last item of the launch advances the ensemble's step counter
-            if (atomicAdd(&P.ctl[1], 1u) + 1 == (unsigned)total) *P.step += P.nsteps;
+            const unsigned d = atomicAdd(&P.done[step * P.nslot + slot], 1u) + 1;
+            // the last slot to finish in the launch's last step advances the
+            // ensemble's step counter (every prologue has read it by then)
+            if (step == P.nsteps - 1 && d == (unsigned)ph.items && atomicAdd(&P.ctl[1], 1u) + 1 == (unsigned)P.nslot)
+                *P.step += P.nsteps;
         }
     }
 }
@@ -298,8 +307,10 @@ int persist_smem(int kind, int len) {
             return host_xlen(len, [](auto n) { return (int)XRShape<decltype(n)::value, 1, true>::SMEM; });
         case PK_PLANE:
             return host_plane(len, [](auto n) { return (int)PlaneShape<decltype(n)::value, kPersistThreads>::SMEM; });
-        case PK_DIV: case PK_VEL:
-            return (int)sizeof(StencilSmem);
+        case PK_DIV:
+            return (int)sizeof(StencilSmem<ST_DIV>);
+        case PK_VEL:
+            return (int)sizeof(StencilSmem<ST_VEL>);
         default:
             return 0;
     }

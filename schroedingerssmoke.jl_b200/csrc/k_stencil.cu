@@ -7,7 +7,7 @@ namespace isf {
 template <int OP>
 __global__ void __launch_bounds__(st::BX* st::TY) k_stencil(StencilArgs a) {
     pdl_enter();
-    __shared__ StencilSmem sm;
+    __shared__ StencilSmem<OP> sm;
     stencil_body<OP>(a, launch_blk(), sm);
 }
 
