@@ -102,7 +102,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--no-matlabport", action="store_true", help="skip the MatlabPort front-end loop")
-    ap.add_argument("--no-tma", action="store_true", help="stage the z pass pencils through registers only")
+    ap.add_argument("--tma", action="store_true", help="stage the z pass pencils with TMA copies into shared memory")
     ap.add_argument("--order-every", type=int, default=0,
                     help="advect through a cell-sorted slot permutation rebuilt every N steps (0: storage order)")
     return ap.parse_args()
@@ -555,7 +555,7 @@ def main():
     P = parts0.shape[0]
     ncells = int(np.prod(c["dims"]))
 
-    isf = pkg.ISF(c["L"], c["dims"], c["hbar"], c["dt"], device=local, flags=pkg.FLAG_NO_TMA if args.no_tma else 0)
+    isf = pkg.ISF(c["L"], c["dims"], c["hbar"], c["dt"], device=local, flags=pkg.FLAG_TMA_Z_PASS if args.tma else 0)
     isf.set_particle_order(args.order_every)
     s = isf.stream
     psi = torch.from_numpy(psi0).to(f"cuda:{local}")
@@ -688,7 +688,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "grid": list(c["dims"]), "torus": list(c["L"]), "hbar": c["hbar"],
-                   "dt": c["dt"], "particles": P, "jet": False, "particle_order_every": args.order_every, "tma_z_pass": not args.no_tma,
+                   "dt": c["dt"], "particles": P, "jet": False, "particle_order_every": args.order_every, "tma_z_pass": args.tma,
                    "l2": "inputs larger than L2: psi 64 MiB + velocity 65 MiB + particles 48 MiB + f 16 MiB + half spectrum 18 MiB",
                    "parallelism": "replicas" if world > 1 else "single"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -20,7 +20,7 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NO_TMA, FLAG_NORMALIZED_WEIGHTS, PHASE_DOT,
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, FLAG_TMA_Z_PASS, PHASE_DOT,
                    PHASE_REFERENCE_SUM, IsfParams, IsfStepArgs, ISFError, check, f3)
 
 __all__ = [

@@ -124,7 +124,7 @@ bool check_params(const isf_params* p, std::string& why) {
         why = "hbar and dt must be finite, dt > 0";
         return false;
     }
-    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN | ISF_FLAG_NO_TMA)) {
+    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN | ISF_FLAG_TMA_Z_PASS)) {
         why = "unknown flags";
         return false;
     }
@@ -235,8 +235,8 @@ int run_schroedinger(isf_handle* h, float* psi, bool norm) {
     xa.psi = reinterpret_cast<float4*>(psi);
     ISF_LAUNCH(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
     ISF_LAUNCH(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
-    // the z pass with TMA-staged pencils where it is built for the length
-    bool tma = !(h->flags & ISF_FLAG_NO_TMA) && zmask_tma_len(h->g.n[2]) && h->g.n[0] % 8 == 0;
+    // the z pass with TMA-staged pencils, when asked for and built for the length
+    bool tma = (h->flags & ISF_FLAG_TMA_Z_PASS) && zmask_tma_len(h->g.n[2]) && h->g.n[0] % 8 == 0;
     if (tma && h->zmap_psi != psi) {
         h->zmap_ok = encode_psi_zmap(&h->zmap, psi, h->g);
         h->zmap_psi = psi;

@@ -70,7 +70,7 @@ struct XShape {
 };
 
 template <int N, int OP, int G, class BarT = CtaBar>
-__device__ __forceinline__ void xpass_body(const XArgs& a, const Blk& bk, unsigned char* smraw,
+__device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned char* smraw,
                                            const BarT& bar = BarT()) {
     using Tr = XTraits<OP>;
     using T = typename Tr::T;
@@ -146,7 +146,7 @@ struct XRShape {
 };
 
 template <int N, int OP, int G, bool KM = false, class BarT = CtaBar>
-__device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsigned char* smraw,
+__device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned char* smraw,
                                            const BarT& bar = BarT()) {
     using T = float2;
     constexpr int C = 16;
@@ -239,16 +239,15 @@ __device__ __forceinline__ void xreal_body(const XArgs& a, const Blk& bk, unsign
                 if (v1) rout[b1 + j] = v.y;
             } else {
                 static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
-                if (v0) {
-                    float4 p0 = psi[b0 + j];
-                    if (use_jet) restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
-                    psi[b0 + j] = gauge4(p0, v.x);
+                // both rows' psi loaded before either is stored (two loads in flight)
+                float4 p0 = v0 ? psi[b0 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                float4 p1 = v1 ? psi[b1 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (use_jet) {
+                    if (v0) restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
+                    if (v1) restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
                 }
-                if (v1) {
-                    float4 p1 = psi[b1 + j];
-                    if (use_jet) restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
-                    psi[b1 + j] = gauge4(p1, v.y);
-                }
+                if (v0) psi[b0 + j] = gauge4(p0, v.x);
+                if (v1) psi[b1 + j] = gauge4(p1, v.y);
             }
         };
         // k-major: the staging aliases the tile, so the first gather must
@@ -303,7 +302,7 @@ struct PlaneShape {
 };
 
 template <int N, class Sh = PlaneShape<N>, class BarT = CtaBar>
-__device__ __forceinline__ void plane_body(const PlaneArgs& a, const Blk& bk, unsigned char* smraw,
+__device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsigned char* smraw,
                                            const BarT& bar = BarT()) {
     constexpr int C = Sh::C, NT = Sh::NT, GT = Sh::GT;
     float2* plane = reinterpret_cast<float2*>(smraw);
@@ -426,7 +425,7 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 }
 
 template <int N, class T, int OP, int G, class BarT = CtaBar>
-__device__ __forceinline__ void yzpass_body(const YZArgs& a, const Blk& bk, unsigned char* smraw,
+__device__ __forceinline__ void yzpass_body(const YZArgs a, const Blk bk, unsigned char* smraw,
                                             const BarT& bar = BarT()) {
     constexpr int C = YZShape<N, T>::C;
     constexpr int NT = Plan<N>::NT;

@@ -54,7 +54,7 @@ struct StencilSmem<ST_VEL> {
 };
 
 template <int OP, class B = CtaBar>
-__device__ __forceinline__ void stencil_body(const StencilArgs& a, const Blk& bk, StencilSmem<OP>& S,
+__device__ __forceinline__ void stencil_body(const StencilArgs a, const Blk bk, StencilSmem<OP>& S,
                                              const B& bar = B()) {
     using namespace st;
     const Grid& g = a.g;

@@ -255,13 +255,14 @@ def test_step_sequences(isfpkg, oracle_mod, cfgs, L, dims):
 @pytest.mark.parametrize("dims", [(64, 32, 128), (32, 16, 64), (16, 8, 256), (24, 8, 96), (40, 12, 192)])
 def test_schroedinger_z_pass_tma_matches_register_staging(isfpkg, dims):
     """The z pass of schroedinger_flow! with its pencils copied into shared
-    memory by the TMA (cp.async.bulk.tensor, double-buffered, bounded
-    mbarrier waits) against the same pass staged through registers
-    (ISF_FLAG_NO_TMA): the arithmetic of a pencil is the same, so psi is
-    bitwise equal, and no wait ran out."""
+    memory by the TMA (ISF_FLAG_TMA_Z_PASS: cp.async.bulk.tensor,
+    double-buffered, bounded mbarrier waits) against the same pass staged
+    through registers
+    (the default): the arithmetic of a pencil is the same, so psi is bitwise
+    equal, and no wait ran out."""
     psi0 = smooth_psi(dims, 12)
     out = []
-    for flags in (0, isfpkg.FLAG_NO_TMA):
+    for flags in (isfpkg.FLAG_TMA_Z_PASS, 0):
         isf = isfpkg.ISF((1, 1, 1), dims, HBAR, DT, flags=flags)
         psi = cuda(psi0)
         for _ in range(2):
