@@ -194,7 +194,7 @@ int join(isf_handle* h) {
 }
 
 void destroy_side(isf_handle* h) {
-    for (cudaEvent_t e : {h->ev_vel, h->ev_side, h->ev_read[0], h->ev_read[1], h->ev_onef})
+    for (cudaEvent_t e : {h->ev_vel, h->ev_side, h->ev_read[0], h->ev_read[1]})
         if (e) cudaEventDestroy(e);
     if (h->side) cudaStreamDestroy(h->side);
     h->side = nullptr;
@@ -230,15 +230,10 @@ YZArgs yzhalf(isf_handle* h, int axis) {
 }
 
 // schroedinger_flow! (+ normalize fused into the last pass when norm != 0)
-int run_schroedinger(isf_handle* h, float* psi, bool norm) { return run_schroedinger_io(h, psi, psi, norm); }
-
-// the same with the x forward pass reading `in` and every pass writing psi
-int run_schroedinger_io(isf_handle* h, const float* in, float* psi, bool norm) {
+int run_schroedinger(isf_handle* h, float* psi, bool norm) {
     XArgs xa = xargs(h);
     xa.psi = reinterpret_cast<float4*>(psi);
-    xa.psi_in = in != psi ? reinterpret_cast<const float4*>(in) : nullptr;
     ISF_LAUNCH(h, launch_xpass(X_PSI_FWD, xa, h->stream), "schroedinger x fwd");
-    xa.psi_in = nullptr;
     ISF_LAUNCH(h, launch_yzpass_psi(YZ_FWD, yzargs(h, psi, 1), h->stream), "schroedinger y fwd");
     // the z pass with TMA-staged pencils, when asked for and built for the length
     bool tma = (h->flags & ISF_FLAG_TMA_Z_PASS) && zmask_tma_len(h->g.n[2]) && h->g.n[0] % 8 == 0;
@@ -282,14 +277,10 @@ int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const c
 
 // pressure_project! with the optional nozzle restriction fused in front:
 // f = div(one-form) -> Poisson solve -> gauge
-int run_projection(isf_handle* h, float* psi, const JetArgs* jet) { return run_projection_io(h, psi, psi, jet); }
-
-// the same with the gauged psi written to `out` (the gauge pass reads psi)
-int run_projection_io(isf_handle* h, float* psi, float* out, const JetArgs* jet) {
+int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
     StencilArgs sa = stargs(h, psi, h->f);
     XArgs xa = xargs(h);
-    xa.psi = reinterpret_cast<float4*>(out);
-    xa.psi_in = out != psi ? reinterpret_cast<const float4*>(psi) : nullptr;
+    xa.psi = reinterpret_cast<float4*>(psi);
     xa.rin = h->f;
     if (jet) {
         sa.jet = *jet;
@@ -426,7 +417,6 @@ int isf_create(const isf_params* p, isf_handle** out) {
         // legacy default stream is ordered after its advection)
         e = cudaStreamCreateWithFlags(&h->side, cudaStreamDefault);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_vel, cudaEventDisableTiming);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_onef, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_side, cudaEventDisableTiming);
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&h->ev_read[i], cudaEventDisableTiming);
         if (e != cudaSuccess) return cleanup(ISF_ERR_CUDA, std::string("isf_create: particle stream: ") + cudaGetErrorString(e));
@@ -463,7 +453,6 @@ int isf_destroy(isf_handle* h) {
         cudaFree(h->tables);
         cudaFree(h->counters);
         cudaFree(h->keep_counts);
-        cudaFree(h->psi_work);
         free_order(h);
         adj_free(h);
         destroy_side(h);
@@ -694,57 +683,29 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
                         (h->order_n != np || h->order_parts != parts || h->order_age >= h->order_every);
     if (resort)
         if (int rc = ensure_order(h, np)) return rc;
-    // With a particle stream the step's psi passes run in the handle's work
-    // copy: the x forward pass reads the caller's psi, and only the last
-    // gauge pass writes it.  The velocity one-form of this step, which reads
-    // psi, then runs on the particle stream beside the next step's passes
-    // (until that step's last gauge pass, which waits for it).
-    const bool overlap = h->side != nullptr;
-    if (overlap && !h->psi_work && cudaMalloc(&h->psi_work, sizeof(float4) * h->g.N) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(h, ISF_ERR_NOMEM, "isf_step: psi work copy: device allocation failed");
-    }
-    float* w = overlap ? reinterpret_cast<float*>(h->psi_work) : psi;
-    auto last_gauge = [&]() -> int {  // before the pass that writes the caller's psi
-        if (overlap && h->onef_pending)
-            ISF_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_onef, 0), "step one-form event");
-        return ISF_OK;
-    };
-    int rc = run_schroedinger_io(h, psi, w, true);  // schroedinger_flow! + normalize_psi
+    int rc = run_schroedinger(h, psi, true);  // schroedinger_flow! + normalize_psi
     if (rc) return rc;
-    if (!a->jet && (rc = last_gauge())) return rc;
-    rc = run_projection_io(h, w, a->jet ? w : psi, nullptr);  // pressure_project!
+    rc = run_projection(h, psi, nullptr);     // pressure_project!
     if (rc) return rc;
     if (a->jet) {
         JetArgs j = make_jet(a->kvec, a->jetmask, a->nozzle_cen, a->nozzle_len, a->nozzle_rad, a->omega_t,
                              a->phase_mode);
-        if ((rc = last_gauge())) return rc;
-        rc = run_projection_io(h, w, psi, &j);  // restrict_velocity! + pressure_project!
+        rc = run_projection(h, psi, &j);  // restrict_velocity! + pressure_project!
         if (rc) return rc;
     }
-    // velocity_one_form!(isf, psi, isf.hbar) + staggered sharp, add_particles!
-    // (before the projections in the reference; the particles are
-    // independent of psi) and staggered_advect!.  With a particle stream they
-    // run there, after this step's psi, while the caller queues the next
-    // step's passes; the velocity grid the advection reads is not written
-    // again until it is done (the one-form alternates between two grids).
+    // velocity_one_form!(isf, psi, isf.hbar) + staggered sharp
+    rc = run_one_form(h, psi, h->g.hbar, 1, "step one_form");
+    if (rc) return rc;
+    // add_particles! (before the projections in the reference; the particles
+    // are independent of psi) and staggered_advect!.  With a particle stream
+    // they run there, after this step's velocity, while the caller queues the
+    // next step's psi passes; the velocity grid they read is not written
+    // again until they are done (run_one_form alternates between two).
     cudaStream_t ps = h->side ? h->side : h->stream;
     const bool emit = a->jet && a->emit_count > 0;
-    if (overlap) {
-        ISF_CUDA(h, cudaEventRecord(h->ev_vel, h->stream), "step psi event");
-        ISF_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_vel, 0), "step psi event");
-        const int nb = h->vcur ^ 1;  // the grid the advection two steps back read, earlier on this stream
-        h->vcur = nb;
-        h->vel = h->vel_buf[nb];
-        StencilArgs va = stargs(h, psi, h->vel);
-        va.hbar = h->g.hbar;
-        va.sharp = 1;
-        ISF_LAUNCH_ON(h, ps, launch_stencil(ST_VEL, va, ps), "step one_form");
-        ISF_CUDA(h, cudaEventRecord(h->ev_onef, h->side), "step one-form event");
-        h->onef_pending = true;
-    } else {
-        rc = run_one_form(h, psi, h->g.hbar, 1, "step one_form");
-        if (rc) return rc;
+    if (h->side && (emit || np > 0)) {
+        ISF_CUDA(h, cudaEventRecord(h->ev_vel, h->stream), "step velocity event");
+        ISF_CUDA(h, cudaStreamWaitEvent(h->side, h->ev_vel, 0), "step velocity event");
     }
     if (emit) {
         EmitArgs e;
@@ -765,7 +726,7 @@ int isf_step(isf_handle* h, float* psi, float* parts, int64_t np, const isf_step
     }
     if (np > 0)
         ISF_LAUNCH_ON(h, ps, launch_advect(h->g, parts, np, h->vel, h->counters, ps, 1, 0, order), "step advect");
-    if (overlap) {
+    if (h->side && (emit || np > 0)) {
         ISF_CUDA(h, cudaEventRecord(h->ev_read[h->vcur], h->side), "step particle event");
         ISF_CUDA(h, cudaEventRecord(h->ev_side, h->side), "step particle event");
         h->side_pending = true;

@@ -56,13 +56,6 @@ struct isf_handle {
     const float* order_parts = nullptr;  // the slot array it was made for
     isf::OrderBufs ord = {};
     long long ord_cap = 0;               // slots the rank / order buffers hold
-    // isf_step on a handle with a particle stream: the step's psi passes run
-    // in psi_work and only the last gauge pass writes the caller's psi, so
-    // the velocity one-form (which reads it) runs on the particle stream
-    // beside the next step's passes; ev_onef: that one-form is done
-    float4* psi_work = nullptr;
-    cudaEvent_t ev_onef = nullptr;
-    bool onef_pending = false;
     // the tensor map of the TMA-staged z pass, for the psi it was encoded for
     isf::CUtensorMapStorage zmap = {};
     const float* zmap_psi = nullptr;
@@ -105,9 +98,7 @@ JetArgs make_jet(const float kvec[3], const uint8_t* mask, const float cen[3], f
 
 // kernel sequences of the reference operators (isf_abi.cu)
 int run_schroedinger(isf_handle* h, float* psi, bool norm);
-int run_schroedinger_io(isf_handle* h, const float* in, float* psi, bool norm);
 int run_projection(isf_handle* h, float* psi, const JetArgs* jet);
-int run_projection_io(isf_handle* h, float* psi, float* out, const JetArgs* jet);
 int run_one_form(isf_handle* h, const float* psi, float hbar, int sharp, const char* site);
 // the y / z transforms and the Laplacian multiply of the Poisson solve on h->F
 int run_poisson_spectral(isf_handle* h, const char* site);

@@ -37,10 +37,6 @@ enum XOp {
 struct XArgs {
     Grid g;
     float4* psi;
-    // psi as the pass reads it, when it differs from psi (the x forward pass
-    // and the gauge pass of isf_step: the caller's psi into a work copy, and
-    // back); null: psi itself
-    const float4* psi_in;
     float2* F;
     const float* rin;
     float* rout;
@@ -89,14 +85,13 @@ __device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned
     // pencils past the end: they read zeros and store nothing
     const bool valid = row < (long long)a.g.n[1] * a.g.n[2];
     float4* __restrict__ psi = a.psi + bk.y * a.bs_psi;
-    const float4* psin = (a.psi_in ? a.psi_in : a.psi) + bk.y * a.bs_psi;
     float2* __restrict__ F = a.F + bk.y * a.bs_F;
     T x[Plan<N>::EMAX];
 
     auto src = [&](int j) -> T {
         if (!valid) return T{};
         if constexpr (Tr::psi_elems) {
-            return psin[rb + j];
+            return psi[rb + j];
         } else {
             return F[rb + j];
         }
@@ -221,7 +216,6 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
         }
         float* __restrict__ rout = a.rout + sim * a.bs_r;
         float4* __restrict__ psi = a.psi + sim * a.bs_psi;
-        const float4* psin = (a.psi_in ? a.psi_in : a.psi) + sim * a.bs_psi;
         const bool use_jet = a.use_jet != 0;
         const JetArgs jet = a.jets ? a.jets[sim] : a.jet;
         auto src = [&](int j) -> T {
@@ -246,8 +240,8 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
             } else {
                 static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
                 // both rows' psi loaded before either is stored (two loads in flight)
-                float4 p0 = v0 ? psin[b0 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                float4 p1 = v1 ? psin[b1 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                float4 p0 = v0 ? psi[b0 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+                float4 p1 = v1 ? psi[b1 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
                 if (use_jet) {
                     if (v0) restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
                     if (v1) restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
