@@ -100,6 +100,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run only the batched-ensemble comparison and print its JSON object (no contract line)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--no-matlabport", action="store_true", help="skip the MatlabPort front-end loop")
     ap.add_argument("--tma", action="store_true", help="stage the z pass pencils with TMA copies into shared memory")
@@ -551,6 +553,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     pkg = ge.load_package()
     cfgs = importlib.import_module(pkg.__name__ + ".configs")
+    if args.batch_only:
+        print(json.dumps(batched_vs_plain(pkg, cfgs, min(args.steps, 100), args.warmup, local)), flush=True)
+        return
     c, psi0, parts0 = setup_workload(cfgs)
     P = parts0.shape[0]
     ncells = int(np.prod(c["dims"]))

@@ -44,7 +44,8 @@ __device__ __forceinline__ float cell_floor_f(float p, float dinv, float d, floa
     const float f1 = floorf(q1);
     if (POW2) return f1;
     const float fr = q1 - f1;
-    return (fr > eps && fr < 1.f - eps) ? f1 : floorf(__fdiv_rn(p, d));
+    if (__builtin_expect(fr > eps && fr < 1.f - eps, 1)) return f1;
+    return floorf(__fdiv_rn(p, d));
 }
 
 // The grid constants the advection needs, copied once into registers (the
@@ -156,30 +157,40 @@ __device__ __forceinline__ int checked(const AdvConst& k, int c, unsigned long l
 #define ISF_IDX(c) (c)
 #endif
 
+// mod.(point, L) for a sample point outside [0, L)^3: out of line, so the
+// common in-box path carries none of its instructions
+static __device__ __noinline__ float3 wrap_box(float3 p, float L0, float L1, float L2) {
+    return make_float3(jl_mod_box(p.x, L0), jl_mod_box(p.y, L1), jl_mod_box(p.z, L2));
+}
+
 // staggered_velocity (parallel.jl:219-246) on the handle's padded velocity
 // grid: seven 16-byte gathers (the cells whose components the reference's
 // twelve samples need).  Interpolation weights are the reference's unnormalised
 // w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
-// clamped to the last cell and counted.
-template <bool POW2, bool NORMW, class B = CtaBar>
+// clamped to the last cell and counted.  INBOX: the caller knows the point
+// lies in [0, L)^3 (the first RK stage of a live particle).
+template <bool POW2, bool NORMW, class B = CtaBar, bool INBOX = false>
 __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigned& clamps, unsigned long long* chk) {
-    float P[3] = {pt.x, pt.y, pt.z};
-    // mod.(point, ph_size): identity for points inside the box (the common case)
-    const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
-                       (pt.z >= 0.f && pt.z < k.L[2]);
-    if (!inbox) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) P[a] = jl_mod_box(P[a], k.L[a]);
+    if (!INBOX) {
+        // mod.(point, ph_size): the identity for points inside the box
+        const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
+                           (pt.z >= 0.f && pt.z < k.L[2]);
+        if (__builtin_expect(!inbox, 0)) pt = wrap_box(pt, k.L[0], k.L[1], k.L[2]);
     }
+    const float P[3] = {pt.x, pt.y, pt.z};
     int i[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         // the cell floor, its clamp and the weight stay in float (integer
-        // values, exact); a NaN point clamps to cell 0 as an int floor would
+        // values, exact).  P lies in [0, L] here, so the floor is >= 0 and
+        // only the upper clamp can act; a NaN point keeps a NaN floor, which
+        // converts to cell 0 and gives NaN weights as the clamped floor did.
         float fl = cell_floor_f<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
-        clamps += (fl > k.nmf[a]) ? 1u : 0u;  // mod rounded up to L
-        fl = fminf(fmaxf(fl, 0.f), k.nmf[a]);
+        if (__builtin_expect(fl > k.nmf[a], 0)) {  // mod rounded up to L
+            ++clamps;
+            fl = k.nmf[a];
+        }
         i[a] = __float2int_rz(fl);
         w[a] = __fsub_rn(P[a], __fmul_rn(fl, k.d[a]));
         if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
@@ -218,7 +229,7 @@ __device__ __forceinline__ void advect_slot(const AdvConst& kc, float* __restric
     if (inside) {
         ++live;
         // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
-        const float3 k1 = stag_vel<POW2, NORMW, B>(kc, p, clamps, chk);
+        const float3 k1 = stag_vel<POW2, NORMW, B, true>(kc, p, clamps, chk);
         float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
         const float3 k2 = stag_vel<POW2, NORMW, B>(kc, q, clamps, chk);
         q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
