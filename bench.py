@@ -146,29 +146,44 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Start sampling every 50 ms; returns once the first sample has
+        arrived (nvidia-smi takes a while to start), so the samples cover the
+        timed region that follows."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.idx), "-lms", "50"], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t0 = time.monotonic()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def stop(self):
+        """Samples taken from start() until one sampling period after the
+        timed region (at least the first sample after it)."""
         if not self.proc:
             return None
-        time.sleep(0.12)
+        t1 = time.monotonic()
+        deadline = t1 + 1.0
+        while time.monotonic() < deadline and not any(t > t1 for t, _ in self.lines):
+            time.sleep(0.01)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.t.join(timeout=2)
+        after = [t for t, _ in self.lines if t > t1]
+        t_end = max(t1 + 0.06, min(after)) if after else t1 + 0.06
+        self.lines = [ln for t, ln in self.lines if self.t0 <= t <= t_end]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:

@@ -178,33 +178,64 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
         if (__builtin_expect(!inbox, 0)) pt = wrap_box(pt, k.L[0], k.L[1], k.L[2]);
     }
     const float P[3] = {pt.x, pt.y, pt.z};
+    // The cell floor, its clamp and the weight stay in float (integer values,
+    // exact).  The common case takes p * (1/d) away from an integer and below
+    // n on all three axes, tested together with one branch; otherwise every
+    // axis takes the exact floor (the IEEE quotient near an integer) and the
+    // upper clamp.  P lies in [0, L] here, so the floor is >= 0 and only the
+    // upper clamp can act; a NaN point keeps a NaN floor, which converts to
+    // cell 0 and gives NaN weights as the clamped floor did.
+    float fl[3];
+    bool fast = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float q1 = P[a] * k.dinv[a];
+        fl[a] = floorf(q1);
+        if (!POW2) {
+            const float fr = q1 - fl[a];
+            fast = fast && fr > k.feps[a] && fr < 1.f - k.feps[a];
+        }
+        fast = fast && !(fl[a] > k.nmf[a]);
+    }
+    if (__builtin_expect(!fast, 0)) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            fl[a] = cell_floor_f<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
+            if (fl[a] > k.nmf[a]) {  // mod rounded up to L
+                ++clamps;
+                fl[a] = k.nmf[a];
+            }
+        }
+    }
     int i[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        // the cell floor, its clamp and the weight stay in float (integer
-        // values, exact).  P lies in [0, L] here, so the floor is >= 0 and
-        // only the upper clamp can act; a NaN point keeps a NaN floor, which
-        // converts to cell 0 and gives NaN weights as the clamped floor did.
-        float fl = cell_floor_f<POW2>(P[a], k.dinv[a], k.d[a], k.feps[a]);
-        if (__builtin_expect(fl > k.nmf[a], 0)) {  // mod rounded up to L
-            ++clamps;
-            fl = k.nmf[a];
-        }
-        i[a] = __float2int_rz(fl);
-        w[a] = __fsub_rn(P[a], __fmul_rn(fl, k.d[a]));
+        i[a] = __float2int_rz(fl[a]);
+        w[a] = __fsub_rn(P[a], __fmul_rn(fl[a], k.d[a]));
         if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
     }
     (void)chk;
-    // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell
+    // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell; the
+    // seven cells as offsets from one base pointer
     const int sy = k.pnx, sz = k.pnxy;
     const int c000 = i[0] + sy * i[1] + sz * i[2];
-    const int c100 = c000 + 1, c010 = c000 + sy, c001 = c000 + sz;
+#ifdef ISF_CHECK
+    const float4* v = k.v;
+    const float4 a000 = ldm<B>(v + ISF_IDX(c000)), a100 = ldm<B>(v + ISF_IDX(c000 + 1));
+    const float4 a010 = ldm<B>(v + ISF_IDX(c000 + sy)), a001 = ldm<B>(v + ISF_IDX(c000 + sz));
+    const float4 a011 = ldm<B>(v + ISF_IDX(c000 + sy + sz)), a101 = ldm<B>(v + ISF_IDX(c000 + 1 + sz));
+    const float4 a110 = ldm<B>(v + ISF_IDX(c000 + 1 + sy));
+#else
     // the reference's 12 samples (parallel.jl:224-234) from 7 cells
-    const float4 a000 = ldm<B>(k.v + ISF_IDX(c000)), a100 = ldm<B>(k.v + ISF_IDX(c100));
-    const float4 a010 = ldm<B>(k.v + ISF_IDX(c010)), a001 = ldm<B>(k.v + ISF_IDX(c001));
-    const float4 a011 = ldm<B>(k.v + ISF_IDX(c010 + sz)), a101 = ldm<B>(k.v + ISF_IDX(c100 + sz));
-    const float4 a110 = ldm<B>(k.v + ISF_IDX(c100 + sy));
+    const float4* b0 = k.v + c000;
+    const float4* by = b0 + sy;
+    const float4* bz = b0 + sz;
+    const float4 a000 = ldm<B>(b0), a100 = ldm<B>(b0 + 1);
+    const float4 a010 = ldm<B>(by), a001 = ldm<B>(bz);
+    const float4 a011 = ldm<B>(by + sz), a101 = ldm<B>(bz + 1);
+    const float4 a110 = ldm<B>(by + 1);
+#endif
     const float x00 = a000.x, x10 = a010.x, x01 = a001.x, x11 = a011.x;
     const float y00 = a000.y, y10 = a100.y, y01 = a001.y, y11 = a101.y;
     const float z00 = a000.z, z10 = a100.z, z01 = a010.z, z11 = a110.z;
