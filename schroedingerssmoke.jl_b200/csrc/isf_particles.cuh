@@ -55,6 +55,7 @@ struct AdvConst {
     float nmf[3];  // n - 1 as a float
     int nm[3];  // n - 1
     int pnx, pnxy;
+    float pnxf, pnxyf;  // the padded strides as floats (cell indices below 2^24 are exact)
     const float4* __restrict__ v;  // (vx, vy, vz, 0) per padded cell
     long long NP;
 };
@@ -72,6 +73,8 @@ __device__ __forceinline__ AdvConst adv_const(const Grid& g, const float* vel) {
     }
     c.pnx = g.pnx;
     c.pnxy = g.pnxy;
+    c.pnxf = (float)g.pnx;
+    c.pnxyf = (float)g.pnxy;
     c.v = reinterpret_cast<const float4*>(vel);
     c.NP = g.NP;
     return c;
@@ -168,13 +171,19 @@ static __device__ __noinline__ float3 wrap_box(float3 p, float L0, float L1, flo
 // twelve samples need).  Interpolation weights are the reference's unnormalised
 // w = p - (i-1) d.  An index that rounds to n (p rounded up to L by mod) is
 // clamped to the last cell and counted.  INBOX: the caller knows the point
-// lies in [0, L)^3 (the first RK stage of a live particle).
-template <bool POW2, bool NORMW, class B = CtaBar, bool INBOX = false>
+// lies in [0, L)^3 (the first RK stage of a live particle).  FIDX: the
+// padded grid has at most 2^24 cells, so the base cell index is formed
+// exactly in float from the floors and converted once.
+template <bool POW2, bool NORMW, class B = CtaBar, bool INBOX = false, bool FIDX = false>
 __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigned& clamps, unsigned long long* chk) {
     if (!INBOX) {
-        // mod.(point, ph_size): the identity for points inside the box
-        const bool inbox = (pt.x >= 0.f && pt.x < k.L[0]) && (pt.y >= 0.f && pt.y < k.L[1]) &&
-                           (pt.z >= 0.f && pt.z < k.L[2]);
+        // mod.(point, ph_size): the identity for points inside the box.  For
+        // x >= +0 and L > 0 the float order is the order of the bit patterns,
+        // so x in [0, L) is one unsigned compare; -0 (in the box as a float)
+        // takes the wrap, which returns it unchanged.
+        const bool inbox = (__float_as_uint(pt.x) < __float_as_uint(k.L[0])) &&
+                           (__float_as_uint(pt.y) < __float_as_uint(k.L[1])) &&
+                           (__float_as_uint(pt.z) < __float_as_uint(k.L[2]));
         if (__builtin_expect(!inbox, 0)) pt = wrap_box(pt, k.L[0], k.L[1], k.L[2]);
     }
     const float P[3] = {pt.x, pt.y, pt.z};
@@ -207,11 +216,9 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
             }
         }
     }
-    int i[3];
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        i[a] = __float2int_rz(fl[a]);
         w[a] = __fsub_rn(P[a], __fmul_rn(fl[a], k.d[a]));
         if (NORMW) w[a] = __fdiv_rn(w[a], k.d[a]);
     }
@@ -219,7 +226,21 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
     // the +1 neighbour mod(i, res) + 1 is the padded plane's next cell; the
     // seven cells as offsets from one base pointer
     const int sy = k.pnx, sz = k.pnxy;
-    const int c000 = i[0] + sy * i[1] + sz * i[2];
+#if defined(ISF_CHECK)
+    constexpr bool kFloatIndex = false;
+#else
+    constexpr bool kFloatIndex = FIDX;
+#endif
+    int c000;
+    int i[3];
+    if constexpr (kFloatIndex) {
+        c000 = __float2int_rz(__fmaf_rn(k.pnxyf, fl[2], __fmaf_rn(k.pnxf, fl[1], fl[0])));
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) i[a] = __float2int_rz(fl[a]);
+        c000 = i[0] + sy * i[1] + sz * i[2];
+    }
+    (void)i;
 #ifdef ISF_CHECK
     const float4* v = k.v;
     const float4 a000 = ldm<B>(v + ISF_IDX(c000)), a100 = ldm<B>(v + ISF_IDX(c000 + 1));
@@ -252,7 +273,7 @@ __device__ __forceinline__ float3 stag_vel(const AdvConst& k, float3 pt, unsigne
 // staggered_advect (parallel.jl:197-216) of slot k: classical RK4 if the
 // particle is inside the open box 0 < p < L, (-1,-1,-1) otherwise (a slot
 // that holds (-1,-1,-1) already is not stored again).
-template <bool POW2, bool NORMW, class B = CtaBar>
+template <bool POW2, bool NORMW, class B = CtaBar, bool FIDX = false>
 __device__ __forceinline__ void advect_slot(const AdvConst& kc, float* __restrict__ parts, int k, float dt, float s6,
                                             unsigned& clamps, unsigned& live, unsigned long long* chk) {
     float3 p = make_float3(parts[3 * k], parts[3 * k + 1], parts[3 * k + 2]);
@@ -260,13 +281,13 @@ __device__ __forceinline__ void advect_slot(const AdvConst& kc, float* __restric
     if (inside) {
         ++live;
         // k2 = p .+ k1 .* dt .* 0.5f0 etc. (parallel.jl:201-212)
-        const float3 k1 = stag_vel<POW2, NORMW, B, true>(kc, p, clamps, chk);
+        const float3 k1 = stag_vel<POW2, NORMW, B, true, FIDX>(kc, p, clamps, chk);
         float3 q = make_float3(p.x + k1.x * dt * 0.5f, p.y + k1.y * dt * 0.5f, p.z + k1.z * dt * 0.5f);
-        const float3 k2 = stag_vel<POW2, NORMW, B>(kc, q, clamps, chk);
+        const float3 k2 = stag_vel<POW2, NORMW, B, false, FIDX>(kc, q, clamps, chk);
         q = make_float3(p.x + k2.x * dt * 0.5f, p.y + k2.y * dt * 0.5f, p.z + k2.z * dt * 0.5f);
-        const float3 k3 = stag_vel<POW2, NORMW, B>(kc, q, clamps, chk);
+        const float3 k3 = stag_vel<POW2, NORMW, B, false, FIDX>(kc, q, clamps, chk);
         q = make_float3(p.x + k3.x * dt, p.y + k3.y * dt, p.z + k3.z * dt);
-        const float3 k4 = stag_vel<POW2, NORMW, B>(kc, q, clamps, chk);
+        const float3 k4 = stag_vel<POW2, NORMW, B, false, FIDX>(kc, q, clamps, chk);
         p.x = p.x + s6 * (k1.x + 2.f * k2.x + 2.f * k3.x + k4.x);
         p.y = p.y + s6 * (k1.y + 2.f * k2.y + 2.f * k3.y + k4.y);
         p.z = p.z + s6 * (k1.z + 2.f * k2.z + 2.f * k3.z + k4.z);

@@ -46,9 +46,21 @@ __global__ void k_emit_soa(float* __restrict__ x, float* __restrict__ y, float* 
 // velocity vel + s * bs_vel, counters + s * kCounterStride.
 // With `order` (a permutation of the np slots, cell-sorted by k_order_*),
 // thread t advects slot order[t]: the arithmetic of every slot is the same,
-// only the traversal changes.
-template <bool POW2, bool NORMW>
-__global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ parts, int np,
+// only the traversal changes.  FIDX: a padded grid of at most 2^24 cells
+// (the base cell index formed in float).
+// ISF_ADV_MINB: resident CTAs per SM the advection is compiled for (caps its
+// registers; 0: ptxas chooses).  At 5 (48 registers, no spills) it runs 409
+// instructions per particle against 427 at the 56 ptxas picks alone.
+#ifndef ISF_ADV_MINB
+#define ISF_ADV_MINB 5
+#endif
+#if ISF_ADV_MINB > 0
+#define ISF_ADV_BOUNDS __launch_bounds__(256, ISF_ADV_MINB)
+#else
+#define ISF_ADV_BOUNDS __launch_bounds__(256)
+#endif
+template <bool POW2, bool NORMW, bool FIDX>
+__global__ void ISF_ADV_BOUNDS k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters, long long bs_vel,
                                                 const int* __restrict__ order) {
@@ -61,7 +73,7 @@ __global__ void __launch_bounds__(256) k_advect(Grid g, float* __restrict__ part
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x)
-        advect_slot<POW2, NORMW>(kc, parts, order ? __ldg(order + t) : t, dt, s6, clamps, live, chk);
+        advect_slot<POW2, NORMW, CtaBar, FIDX>(kc, parts, order ? __ldg(order + t) : t, dt, s6, clamps, live, chk);
     if (counters) {
         // block-aggregated counters: one atomic per CTA and counter
         __shared__ unsigned red[2][8];
@@ -503,7 +515,8 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
         int dev = 0, sms = 0, per = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false, false>, blk, 0) != cudaSuccess || per < 1)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false, false, true>, blk, 0) != cudaSuccess ||
+            per < 1)
             return cudaErrorInvalidValue;
         resident = sms * per;
     }
@@ -511,15 +524,16 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     if (ISF_ADVECT_WAVES > 0 && b > (long long)ISF_ADVECT_WAVES * resident) b = (long long)ISF_ADVECT_WAVES * resident;
     const dim3 grid((unsigned)b, (unsigned)nsim);
     const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
-    if (g.norm_w)
-        return pow2 ? launch_pdl(k_advect<true, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
-                                 order)
-                    : launch_pdl(k_advect<false, true>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
-                                 order);
-    return pow2 ? launch_pdl(k_advect<true, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
-                             order)
-                : launch_pdl(k_advect<false, false>, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel,
-                             order);
+    const bool fidx = g.NP <= (1LL << 24);
+    auto go = [&](auto kernel) {
+        return launch_pdl(kernel, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel, order);
+    };
+    if (g.norm_w) {
+        if (pow2) return fidx ? go(k_advect<true, true, true>) : go(k_advect<true, true, false>);
+        return fidx ? go(k_advect<false, true, true>) : go(k_advect<false, true, false>);
+    }
+    if (pow2) return fidx ? go(k_advect<true, false, true>) : go(k_advect<true, false, false>);
+    return fidx ? go(k_advect<false, false, true>) : go(k_advect<false, false, false>);
 }
 
 cudaError_t launch_order_count(const Grid& g, const float* parts, long long np, const OrderBufs& b, cudaStream_t s) {
