@@ -1,5 +1,7 @@
 // Particle kernels: seeded emission (add_particles!) and RK4 advection on the
 // staggered velocity (staggered_advect!).
+#include <cstdlib>
+
 #include "isf_launch.h"
 #include "isf_particles.cuh"
 
@@ -524,7 +526,11 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     if (ISF_ADVECT_WAVES > 0 && b > (long long)ISF_ADVECT_WAVES * resident) b = (long long)ISF_ADVECT_WAVES * resident;
     const dim3 grid((unsigned)b, (unsigned)nsim);
     const bool pow2 = g.d_pow2[0] && g.d_pow2[1] && g.d_pow2[2];
-    const bool fidx = g.NP <= (1LL << 24);
+    // the float base-cell index needs the padded grid below 2^24 cells; the
+    // environment variable ISF_ADVECT_INT_INDEX (read once) forces the
+    // integer index, so tests can compare the two paths on one grid
+    static const bool force_int = std::getenv("ISF_ADVECT_INT_INDEX") != nullptr;
+    const bool fidx = !force_int && g.NP <= (1LL << 24);
     auto go = [&](auto kernel) {
         return launch_pdl(kernel, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel, order);
     };

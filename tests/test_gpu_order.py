@@ -96,3 +96,50 @@ def test_ordered_steps_are_bitwise_storage_order(isfpkg, cfgs, jet):
     assert np.array_equal(psi_a.view(np.uint32), psi_b.view(np.uint32))
     assert np.array_equal(parts_a.view(np.uint32), parts_b.view(np.uint32))
     assert live_a == live_b
+
+
+_INDEX_RUN = r"""
+import hashlib, sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+sys.path.insert(0, sys.argv[2])
+import __graft_entry__ as ge
+from helpers import smooth_psi
+pkg = ge.load_package()
+L, dims = (4, 2, 2), (64, 32, 32)
+rng = np.random.default_rng(7)
+p0 = (rng.uniform(-0.05, 1.05, (30000, 3)) * np.asarray(L)).astype(np.float32)
+p0[:16] = np.asarray(L, np.float32) * np.float32(0.999999)   # near the upper faces
+isf = pkg.ISF(L, dims, float(np.float32(0.1)), float(np.float32(1 / 48)))
+psi = torch.tensor(smooth_psi(dims, 6), dtype=torch.float32, device="cuda")
+parts = torch.tensor(p0, device="cuda")
+cnt = []
+for _ in range(12):
+    pkg.step(isf, psi, parts, None)
+    c = isf.counters(reset=True)
+    cnt.append((c["live"], c["clamp_events"]))
+isf.sync()
+print(hashlib.md5(parts.cpu().numpy().tobytes()).hexdigest(), cnt)
+"""
+
+
+def test_float_and_integer_cell_index_agree_bitwise():
+    """The advection forms the base cell index from the three floors in float
+    (exact below 2^24 padded cells) or in integers (larger grids).  The same
+    12 steps, in two processes, one forced onto the integer index: the
+    positions and the live / clamp counters agree bitwise."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    tests = os.path.dirname(os.path.abspath(__file__))
+    outs = []
+    for force in (False, True):
+        env = dict(os.environ)
+        env.pop("ISF_ADVECT_INT_INDEX", None)
+        if force:
+            env["ISF_ADVECT_INT_INDEX"] = "1"
+        r = subprocess.run([sys.executable, "-c", _INDEX_RUN, repo, tests], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(r.stdout.strip().splitlines()[-1])
+    assert outs[0] == outs[1], outs
