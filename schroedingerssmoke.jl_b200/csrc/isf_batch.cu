@@ -115,7 +115,8 @@ struct isf_batch {
     unsigned* d_ctl = nullptr;
     int* d_status = nullptr;
     long long spin_limit = 1LL << 22;
-    int pgrid = 0, psmem = 0;
+    int pgrid = 0, psmem = 0, psms = 0;  // persistent grid, its shared memory per block, the SMs it spans
+    int dstride = 0, tiles_per_step = 0; // completion counters and tiles per step
     int preps = 1;                 // tuned: tiles per virtual CTA and item
     std::map<int, cudaGraphExec_t> pgraphs;
 };
@@ -536,15 +537,50 @@ int build_plan(isf_batch* b, int reps, int blocks_per_sm_cap) {
                 slot_of[ci].push_back((int)ph.size());
                 ph.push_back(chains[ci][j]);
             }
-    for (size_t ci = 0; ci < chains.size(); ++ci)
-        for (size_t j = 0; j < chains[ci].size(); ++j) {
+    // Dependencies: each pass waits for the pass before it in its class's
+    // chain, and a few also wait for a pass of the previous step, so that
+    // step n's advection runs beside step n+1's psi passes:
+    //   prologue(n+1) after the last pass of step n that reads the jet and
+    //     emission arguments it rewrites (the jet projection's gauge pass);
+    //   x fwd(n+1), which transforms psi in place, after the one-form of step
+    //     n, the last reader of psi;
+    //   emission and one-form of step n+1, which write the particles and the
+    //     velocity grid, after the advection of step n.
+    for (size_t ci = 0; ci < chains.size(); ++ci) {
+        const std::vector<PPhase>& ch = chains[ci];
+        auto slot = [&](int kind, bool last) {
+            int found = -1;
+            for (size_t j = 0; j < ch.size(); ++j)
+                if (ch[j].kind == kind) {
+                    found = slot_of[ci][j];
+                    if (!last) break;
+                }
+            return found;
+        };
+        const bool jet = b->cls[ci].key.jet;
+        const int vel = slot(PK_VEL, true), adv = slot(PK_ADVECT, true);
+        const int jet_gauge = jet ? slot(PK_XR_INV_GAUGE, true) : -1;
+        for (size_t j = 0; j < ch.size(); ++j) {
             PPhase& p = ph[slot_of[ci][j]];
             p.dep = j > 0 ? slot_of[ci][j - 1] : -1;
-            p.dep_prev = j == 0 ? slot_of[ci].back() : -1;
+            switch (p.kind) {
+                case PK_PROLOGUE: p.dep_prev = jet_gauge; break;
+                case PK_X_FWD: p.dep_prev = vel; break;
+                case PK_EMIT: case PK_VEL: p.dep_prev = adv; break;
+                default: p.dep_prev = -1; break;
+            }
         }
-    int smem = 0;
+    }
+    int smem = 0, dstride = 0, tiles_per_step = 0;
     std::vector<int> start(1, 0);
     for (PPhase& p : ph) {
+        // completion groups: the class's simulations when the tiles are
+        // simulation-major (every pass but the prologue), else one
+        p.nsg = (p.kind != PK_PROLOGUE && p.nsim > 1 && p.tiles % p.nsim == 0) ? p.nsim : 1;
+        p.tps = p.tiles / p.nsg;
+        p.doff = dstride;
+        dstride += p.nsg;
+        tiles_per_step += p.tiles;
         p.vblk = persist_vblk(p.kind, p.len);
         // a virtual CTA is whole warps (its named barrier counts threads in warps)
         if (p.vblk < 32 || p.vblk % 32 != 0 || p.vblk > kPersistThreads)
@@ -575,8 +611,11 @@ int build_plan(isf_batch* b, int reps, int blocks_per_sm_cap) {
     B_CUDA(b, cudaMemset(b->d_status, 0, 4 * sizeof(int)), "persistent plan");
     b->phases = ph;
     b->slot_start = start;
+    b->dstride = dstride;
+    b->tiles_per_step = tiles_per_step;
     b->psmem = smem;
     b->pgrid = sms * bps;
+    b->psms = sms;
     b->preps = reps;
     return ISF_OK;
 }
@@ -590,6 +629,8 @@ PPlan make_plan(const isf_batch* b, int nsteps) {
     p.items_per_step = b->slot_start.back();
     p.nsteps = nsteps;
     p.done = b->d_done;
+    p.dstride = b->dstride;
+    p.tiles_per_step = b->tiles_per_step;
     p.ctl = b->d_ctl;
     p.status = b->d_status;
     p.spin_limit = b->spin_limit;
@@ -604,8 +645,7 @@ PPlan make_plan(const isf_batch* b, int nsteps) {
 
 // queue nsteps persistent steps on s: zero the item counters, one launch
 cudaError_t queue_persist(isf_batch* b, int nsteps, cudaStream_t s) {
-    const size_t nslot = b->phases.size();
-    cudaError_t e = cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * nslot * nsteps, s);
+    cudaError_t e = cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * (size_t)b->dstride * nsteps, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ctl, 0, 2 * sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, 4 * sizeof(int), s);
     if (e == cudaSuccess) e = launch_persist(make_plan(b, nsteps), b->pgrid, b->psmem, s);
@@ -620,7 +660,7 @@ int ensure_done(isf_batch* b, long long nsteps) {
     b->d_done = nullptr;
     b->done_cap = 0;
     const long long cap = std::max<long long>(nsteps, 128);
-    if (cudaMalloc(&b->d_done, sizeof(unsigned) * b->phases.size() * cap) != cudaSuccess) {
+    if (cudaMalloc(&b->d_done, sizeof(unsigned) * (size_t)b->dstride * cap) != cudaSuccess) {
         cudaGetLastError();
         return bfail(b, ISF_ERR_NOMEM, "persistent kernel: device allocation failed");
     }
@@ -640,8 +680,12 @@ int tune_persist(isf_batch* b, bool tune) {
         float best = 1e30f;
         int rc = ISF_OK;
         for (int reps : {1, 2, 4}) {
-            for (int bps : {2, 1}) {
+            int tried = 0;  // blocks per SM already timed at this reps (the cap can clamp a candidate)
+            for (int bps : {4, 3, 2, 1}) {
                 if ((rc = build_plan(b, reps, bps)) != ISF_OK) break;
+                const int eff = b->pgrid / std::max(1, b->psms);
+                if (tried & (1 << eff)) continue;
+                tried |= 1 << eff;
                 if ((rc = ensure_done(b, 3)) != ISF_OK) break;
                 cudaError_t e = queue_persist(b, 3, b->stream);  // warm-up
                 if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);

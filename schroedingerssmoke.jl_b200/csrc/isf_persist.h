@@ -10,7 +10,9 @@
 // step pass by pass with the classes interleaved, so a phase's predecessor
 // in its class's chain always has smaller item numbers: a block that waits
 // for it waits only on items already taken by running blocks, which never
-// wait on later ones.  Every wait is bounded: after `spin_limit` polls the
+// wait on later ones.  A phase's tiles are simulation-major and the
+// simulations are independent, so completion is counted per (step, slot,
+// simulation): an item waits only for the simulations its tiles belong to.  Every wait is bounded: after `spin_limit` polls the
 // block records ISF_ERR_TIMEOUT, the slot and the step in the status word,
 // and every block stops at its next item.
 #pragma once
@@ -50,6 +52,8 @@ struct PPhase {
     int gx, gy;         // tile t -> block (t % gx, (t / gx) % gy, t / (gx gy))
     int dep;            // slot of the same step this phase waits for (-1: none)
     int dep_prev;       // slot of the previous step it waits for (-1: none)
+    int nsg, tps;       // completion groups (the class's simulations; 1 for the prologue) and tiles per group
+    int doff;           // first completion counter of this slot within a step
     int smem_v;         // shared memory bytes of one virtual CTA
     int pow2, normw;    // advection variants
     // arguments of the pass (the member of its kind)
@@ -69,8 +73,10 @@ struct PPlan {
     const PPhase* ph;        // nslot phases, in slot order
     const int* slot_start;   // nslot + 1: first item of each slot within a step
     int nslot, items_per_step, nsteps;
-    unsigned* done;          // nsteps x nslot items finished (zeroed before the launch)
-    unsigned* ctl;           // [0] next item, [1] slots finished in the last step (zeroed before the launch)
+    int dstride;             // completion counters per step (the slots' nsg summed)
+    int tiles_per_step;      // tiles of all slots of one step
+    unsigned* done;          // nsteps x dstride tiles finished per (slot, simulation) (zeroed before the launch)
+    unsigned* ctl;           // [0] next item, [1] tiles finished in the last step (zeroed before the launch)
     int* status;             // [0] error code, [1] slot, [2] step, [3] a flag nothing sets (zeroed)
     long long spin_limit;    // polls of one wait before it gives up
     int stall;               // 1: the first dependent item also waits for status[3] (a timeout by construction)

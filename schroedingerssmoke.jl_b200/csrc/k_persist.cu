@@ -70,6 +70,20 @@ __device__ void report(const PPlan& P, int slot, int step) {
     __threadfence();
 }
 
+// Wait until phase q of step `step` has finished the tiles that an item in
+// completion groups [g0, g1] of a phase with nsg groups depends on: the same
+// simulations when both count per simulation, else all of q.
+__device__ bool wait_groups(const PPlan& P, const PPhase& q, int step, int nsg, int g0, int g1) {
+    const unsigned* dn = P.done + (size_t)step * P.dstride + q.doff;
+    if (q.nsg != nsg) {
+        g0 = 0;
+        g1 = q.nsg - 1;
+    }
+    for (int g = g0; g <= g1; ++g)
+        if (!bounded_wait(&dn[g], (unsigned)q.tps, P.spin_limit, P.status)) return false;
+    return true;
+}
+
 // one tile (virtual CTA) of a phase
 __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int tile, int step, int vt,
                                          unsigned char* sm, const NamedBar& bar) {
@@ -179,7 +193,14 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
 
 }  // namespace
 
-__global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
+// resident blocks per SM the kernel is compiled for (caps its registers at
+// 65536 / (256 x ISF_PERSIST_MINB)): at 3 (80 registers, the larger bodies
+// spill) the 64-jet ensemble step takes 1.27 ms against 1.39 ms at 2 (128
+// registers) and 1.40 ms at 4 (64 registers)
+#ifndef ISF_PERSIST_MINB
+#define ISF_PERSIST_MINB 3
+#endif
+__global__ void __launch_bounds__(kPersistThreads, ISF_PERSIST_MINB) k_persist(PPlan P) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int s_item, s_go;
     __shared__ int s_start[kPersistMaxSlots + 1];  // the slot table, searched per item
@@ -208,14 +229,14 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
         }
         const int slot = lo;
         const PPhase& ph = P.ph[slot];
+        // the item's tiles [t0, t1) and the completion groups (simulations) they lie in
+        const int t0 = (r - s_start[slot]) * ph.reps * ph.vper;
+        const int t1 = min(ph.tiles, t0 + ph.reps * ph.vper);
+        const int g0 = t0 / ph.tps, g1 = (t1 - 1) / ph.tps;
         if (threadIdx.x == 0) {
             bool ok = true;
-            if (ph.dep >= 0)
-                ok = bounded_wait(&P.done[step * P.nslot + ph.dep], (unsigned)P.ph[ph.dep].items, P.spin_limit,
-                                  P.status);
-            if (ok && step > 0 && ph.dep_prev >= 0)
-                ok = bounded_wait(&P.done[(step - 1) * P.nslot + ph.dep_prev], (unsigned)P.ph[ph.dep_prev].items,
-                                  P.spin_limit, P.status);
+            if (ph.dep >= 0) ok = wait_groups(P, P.ph[ph.dep], step, ph.nsg, g0, g1);
+            if (ok && step > 0 && ph.dep_prev >= 0) ok = wait_groups(P, P.ph[ph.dep_prev], step - 1, ph.nsg, g0, g1);
             // the stall switch: an item with a dependency also waits for
             // status[3], which nothing writes, so the wait runs out
             if (ok && P.stall && (ph.dep >= 0 || (step > 0 && ph.dep_prev >= 0)))
@@ -238,11 +259,14 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_persist(PPlan P) {
         }
         __syncthreads();  // every virtual CTA of the item is done
         if (threadIdx.x == 0) {
-            __threadfence();  // release: the item's writes before its count
-            const unsigned d = atomicAdd(&P.done[step * P.nslot + slot], 1u) + 1;
-            // the last slot to finish in the launch's last step advances the
+            __threadfence();  // release: the item's writes before its counts
+            unsigned* dn = P.done + (size_t)step * P.dstride + ph.doff;
+            for (int g = g0; g <= g1; ++g)
+                atomicAdd(&dn[g], (unsigned)(min(t1, (g + 1) * ph.tps) - max(t0, g * ph.tps)));
+            // the item that completes the launch's last step advances the
             // ensemble's step counter (every prologue has read it by then)
-            if (step == P.nsteps - 1 && d == (unsigned)ph.items && atomicAdd(&P.ctl[1], 1u) + 1 == (unsigned)P.nslot)
+            if (step == P.nsteps - 1 &&
+                atomicAdd(&P.ctl[1], (unsigned)(t1 - t0)) + (unsigned)(t1 - t0) == (unsigned)P.tiles_per_step)
                 *P.step += P.nsteps;
         }
     }
