@@ -375,8 +375,10 @@ ISF_API int isf_batch_sync(isf_batch* b);
  * Its blocks take work items in order from one counter: an item is a few
  * CTAs' worth of one pass of one class (the passes of isf_step, the same
  * arithmetic, so results are bitwise those of the per-step graph and of
- * isf_step).  A pass waits on the device for the pass before it in its
- * class's chain with a bounded poll: after spin_limit polls (<= 0: the
+ * isf_step).  A pass waits on the device, per simulation, for the pass
+ * before it in its class's chain (and a few passes for one of the previous
+ * step, so that a step's advection overlaps the next step's psi passes)
+ * with a bounded poll: after spin_limit polls (<= 0: the
  * default, 2^22, about a second) the kernel records ISF_ERR_TIMEOUT, every
  * block stops at its next item, and isf_batch_sync returns ISF_ERR_TIMEOUT
  * naming the pass; the state is then partly stepped.  ISF_PERSIST_STALL adds
