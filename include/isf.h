@@ -63,6 +63,13 @@ enum {
      * them into registers; same results, bitwise.  Off by default: on the
      * 256 x 128 x 128 step it measured 38.8 us against 37.6 us */
     ISF_FLAG_TMA_Z_PASS = 4,
+    /* test switch of the TMA z pass: after its first tile has arrived, every
+     * CTA also waits on a flag that nothing sets (counter 13, always 0), so
+     * the bounded wait runs out.  Each CTA counts the timeout in counter 14,
+     * waits (bounded) for its copy still in flight and returns: psi is left
+     * partly transformed and the context stays usable.  Only with
+     * ISF_FLAG_TMA_Z_PASS; for testing the timeout path. */
+    ISF_FLAG_TMA_Z_STALL = 8,
 };
 
 /* jet phase: reference tuple_dot(k, x) = sum(k .+ x) (src/particles.jl:1,15)
@@ -203,9 +210,10 @@ ISF_API int isf_fft3(isf_handle* h, float* data_dev, int32_t sign);
  * events (staggered_velocity index rounded to n+1), [1] live particles; in a
  * bounds-checking build (-DISF_CHECK) [2] rejected gather indices, [3] the
  * first of them and [4..11] its cell indices, two neighbour indices and strides;
+ * [13] always 0 (the flag ISF_FLAG_TMA_Z_STALL waits on);
  * [14] waits of the TMA-staged Schroedinger z pass (ISF_FLAG_TMA_Z_PASS)
  * that ran out (its CTA then stops; 0 unless a copy stalled for about half
- * a second); [15] non-finite
+ * a second, or ISF_FLAG_TMA_Z_STALL); [15] non-finite
  * psi cells after the last isf_step of a handle made with ISF_FLAG_CHECK_NAN.
  * Synchronises the handle's stream. */
 ISF_API int isf_counters(isf_handle* h, uint64_t* out, int32_t n, int32_t reset);

@@ -20,7 +20,8 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, FLAG_TMA_Z_PASS, PHASE_DOT,
+from ._lib import (EMIT_CYLINDER, EMIT_DISC, EMIT_RING, EMIT_RING_PLANE, FLAG_CHECK_NAN, FLAG_NORMALIZED_WEIGHTS, FLAG_TMA_Z_PASS,
+                   FLAG_TMA_Z_STALL, PHASE_DOT,
                    PHASE_REFERENCE_SUM, IsfParams, IsfStepArgs, ISFError, check, f3)
 
 __all__ = [

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libisf.so")
 
 ISF_OK, ISF_ERR_INVALID, ISF_ERR_CUDA, ISF_ERR_NOMEM, ISF_ERR_NAN, ISF_ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
 PERSIST_ON, PERSIST_STALL = 1, 2
-FLAG_NORMALIZED_WEIGHTS, FLAG_CHECK_NAN, FLAG_TMA_Z_PASS = 1, 2, 4
+FLAG_NORMALIZED_WEIGHTS, FLAG_CHECK_NAN, FLAG_TMA_Z_PASS, FLAG_TMA_Z_STALL = 1, 2, 4, 8
 PHASE_REFERENCE_SUM, PHASE_DOT = 0, 1
 EMIT_RING, EMIT_DISC, EMIT_CYLINDER, EMIT_RING_PLANE = 0, 1, 2, 3
 

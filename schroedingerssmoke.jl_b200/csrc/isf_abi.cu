@@ -124,7 +124,7 @@ bool check_params(const isf_params* p, std::string& why) {
         why = "hbar and dt must be finite, dt > 0";
         return false;
     }
-    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN | ISF_FLAG_TMA_Z_PASS)) {
+    if (p->flags & ~(ISF_FLAG_NORMALIZED_WEIGHTS | ISF_FLAG_CHECK_NAN | ISF_FLAG_TMA_Z_PASS | ISF_FLAG_TMA_Z_STALL)) {
         why = "unknown flags";
         return false;
     }
@@ -243,7 +243,8 @@ int run_schroedinger(isf_handle* h, float* psi, bool norm) {
     }
     tma = tma && h->zmap_ok;
     if (tma)
-        ISF_LAUNCH(h, launch_zmask_tma(h->zmap, yzargs(h, psi, 2), kTmaWaitLimit, h->counters + 14, h->stream),
+        ISF_LAUNCH(h, launch_zmask_tma(h->zmap, yzargs(h, psi, 2), kTmaWaitLimit, h->counters + 14,
+                                       (h->flags & ISF_FLAG_TMA_Z_STALL) ? h->counters + 13 : nullptr, h->stream),
                    "schroedinger z mask");
     else
         ISF_LAUNCH(h, launch_yzpass_psi(YZ_MASK, yzargs(h, psi, 2), h->stream), "schroedinger z mask");

@@ -62,8 +62,10 @@ struct alignas(64) CUtensorMapStorage {
 };
 bool zmask_tma_len(int n);
 bool encode_psi_zmap(CUtensorMapStorage* out, const float* psi, const Grid& g);
+// stall: null, or a counter that nothing sets, which every CTA also waits on
+// after its first tile (the timeout test)
 cudaError_t launch_zmask_tma(const CUtensorMapStorage& map, const YZArgs& a, long long limit, unsigned long long* err,
-                             cudaStream_t s);
+                             const unsigned long long* stall, cudaStream_t s);
 
 // z-marching stencils of the one-form (k_stencil.cu)
 enum StOp { ST_DIV = 0, ST_VEL = 1 };

@@ -15,7 +15,8 @@
 // The tensor map covers this GPU's own psi only; there is no cluster
 // multicast.  Every mbarrier wait is bounded: a wait that runs out adds one
 // to the error counter, drains (again bounded) the copy still in flight,
-// and the CTA returns.
+// and the CTA returns.  A test switch (stall) makes the first wait run out
+// on purpose after its copy has arrived.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -56,6 +57,17 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     return false;
 }
 
+// poll a flag in global memory until it is non-zero, at most `limit` times
+__device__ __forceinline__ bool flag_wait(const unsigned long long* flag, long long limit) {
+    for (long long k = 0; k < limit; ++k) {
+        unsigned long long v;
+        asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(flag) : "memory");
+        if (v != 0) return true;
+        __nanosleep(128);
+    }
+    return false;
+}
+
 // 2D tile copy global -> shared, completion counted on bar (x innermost, in elements)
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
     asm volatile(
@@ -78,7 +90,7 @@ struct ZT {
 template <int N>
 __global__ void __launch_bounds__(ZT<N>::BLK, ZT<N>::MINB)
     k_zmask_tma(const __grid_constant__ CUtensorMap map, YZArgs a, int ntiles, long long limit,
-                unsigned long long* __restrict__ err) {
+                unsigned long long* __restrict__ err, const unsigned long long* stall) {
     using Z = ZT<N>;
     constexpr int C = Z::C, TILE = Z::TILE;
     extern __shared__ unsigned char smraw[];
@@ -117,7 +129,10 @@ __global__ void __launch_bounds__(ZT<N>::BLK, ZT<N>::MINB)
         const int tt = blockIdx.x + k * gridDim.x;
         if (tt >= ntiles) break;
         const int b = k & 1;
-        const bool ok = mbar_wait(&bars[b], (unsigned)((k >> 1) & 1), limit);
+        bool ok = mbar_wait(&bars[b], (unsigned)((k >> 1) & 1), limit);
+        // the timeout test: the first tile has arrived, then a flag that
+        // nothing sets is awaited (briefly), so the error path runs
+        if (stall != nullptr && k == 0 && tid == 0) ok = ok && flag_wait(stall, 256);
         if (__syncthreads_or(ok ? 0 : 1)) {
             // a copy that did not arrive: count it, wait (bounded) for the
             // other buffer's copy if one is in flight, and return
@@ -153,7 +168,7 @@ __global__ void __launch_bounds__(ZT<N>::BLK, ZT<N>::MINB)
 
 template <int N>
 cudaError_t launch_zt(const CUtensorMap& map, const YZArgs& a, long long limit, unsigned long long* err,
-                      cudaStream_t s) {
+                      const unsigned long long* stall, cudaStream_t s) {
     using Z = ZT<N>;
     static int grid_cap = 0;  // CTAs resident on the device
     static std::once_flag once;
@@ -170,7 +185,7 @@ cudaError_t launch_zt(const CUtensorMap& map, const YZArgs& a, long long limit, 
     if (setup != cudaSuccess) return setup;
     const int ntiles = (a.row / Z::C) * a.g.n[1];
     const int grid = ntiles < grid_cap ? ntiles : grid_cap;
-    return launch_pdl(k_zmask_tma<N>, dim3(grid), dim3(Z::BLK), Z::SMEM, s, map, a, ntiles, limit, err);
+    return launch_pdl(k_zmask_tma<N>, dim3(grid), dim3(Z::BLK), Z::SMEM, s, map, a, ntiles, limit, err, stall);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -207,14 +222,14 @@ bool encode_psi_zmap(CUtensorMapStorage* out, const float* psi, const Grid& g) {
 }
 
 cudaError_t launch_zmask_tma(const CUtensorMapStorage& map, const YZArgs& a, long long limit, unsigned long long* err,
-                             cudaStream_t s) {
+                             const unsigned long long* stall, cudaStream_t s) {
     const CUtensorMap& m = reinterpret_cast<const CUtensorMap&>(map);
     switch (a.g.n[2]) {
-        case 64: return launch_zt<64>(m, a, limit, err, s);
-        case 96: return launch_zt<96>(m, a, limit, err, s);
-        case 128: return launch_zt<128>(m, a, limit, err, s);
-        case 192: return launch_zt<192>(m, a, limit, err, s);
-        case 256: return launch_zt<256>(m, a, limit, err, s);
+        case 64: return launch_zt<64>(m, a, limit, err, stall, s);
+        case 96: return launch_zt<96>(m, a, limit, err, stall, s);
+        case 128: return launch_zt<128>(m, a, limit, err, stall, s);
+        case 192: return launch_zt<192>(m, a, limit, err, stall, s);
+        case 256: return launch_zt<256>(m, a, limit, err, stall, s);
         default: return cudaErrorInvalidValue;
     }
 }

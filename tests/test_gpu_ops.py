@@ -274,6 +274,33 @@ def test_schroedinger_z_pass_tma_matches_register_staging(isfpkg, dims):
     assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
 
 
+def test_tma_z_pass_wait_times_out_and_the_gpu_keeps_answering(isfpkg):
+    """ISF_FLAG_TMA_Z_STALL makes every CTA of the TMA z pass wait, after its
+    first tile has arrived, on a flag that nothing sets: the bounded wait runs
+    out, each CTA counts it in counter 14, waits for its copy still in flight
+    and returns.  No fault and no trap: the same handle and a fresh one then
+    run the pass normally and match the register-staged pass."""
+    dims = (32, 16, 64)
+    psi0 = smooth_psi(dims, 12)
+    isf = isfpkg.ISF((1, 1, 1), dims, HBAR, DT, flags=isfpkg.FLAG_TMA_Z_PASS | isfpkg.FLAG_TMA_Z_STALL)
+    psi = cuda(psi0)
+    isfpkg.schroedinger_flow(isf, psi)
+    isf.sync()
+    c = isf.counters(reset=True)
+    assert c["wait_timeouts"] > 0, c
+    isf.close()
+    out = []
+    for flags in (isfpkg.FLAG_TMA_Z_PASS, 0):
+        h = isfpkg.ISF((1, 1, 1), dims, HBAR, DT, flags=flags)
+        p = cuda(psi0)
+        isfpkg.schroedinger_flow(h, p)
+        h.sync()
+        assert h.counters()["wait_timeouts"] == 0
+        out.append(p.cpu().numpy())
+        h.close()
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+
+
 def test_invalid_arguments(isfpkg):
     with pytest.raises(isfpkg.ISFError):
         isfpkg.ISF((1, 1, 1), (22, 8, 8), HBAR, DT)  # 22 = 2 x 11: no radix plan
