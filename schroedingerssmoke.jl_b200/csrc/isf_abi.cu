@@ -292,7 +292,7 @@ int run_projection(isf_handle* h, float* psi, const JetArgs* jet) {
     ISF_LAUNCH(h, launch_stencil(ST_DIV, sa, h->stream), "projection div");
     ISF_LAUNCH(h, launch_xreal(XR_FWD, xa, h->stream), "projection x fwd");
     if (int rc = run_poisson_spectral(h, "projection")) return rc;
-    ISF_LAUNCH(h, launch_xreal(XR_INV_GAUGE, xa, h->stream), "projection x inv + gauge");
+    ISF_LAUNCH(h, launch_xreal(jet ? XR_INV_GAUGE_JET : XR_INV_GAUGE, xa, h->stream), "projection x inv + gauge");
     return ISF_OK;
 }
 

@@ -242,7 +242,7 @@ cudaError_t class_projection(const BatchClass& c, const JetArgs* jets, cudaStrea
         if ((e = launch_yzpass_c(YZ_FAC, byz(c, true, 2, c.tiles[ISF_TILE_Z_HALF]), s)) != cudaSuccess) return e;
         if ((e = launch_yzpass_c(YZ_INV, byz(c, true, 1, c.tiles[ISF_TILE_Y_HALF]), s)) != cudaSuccess) return e;
     }
-    return launch_xreal(XR_INV_GAUGE, xa, s);
+    return launch_xreal(jets ? XR_INV_GAUGE_JET : XR_INV_GAUGE, xa, s);
 }
 
 // the simloop body of isf_step for every simulation of the class

@@ -132,7 +132,10 @@ __global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
 //                           (k_poisson_plane); A and B of a row pair are
 //                           neighbours, moved as one 16-byte vector, with the
 //                           lanes running over row pairs.
-enum XROp { XR_FWD = 0, XR_INV_GAUGE = 1, XR_INV_REAL = 2 };
+//   XR_INV_GAUGE_JET  the gauge with psi restricted in the nozzle first (use_jet):
+//                 a separate op so that the plain gauge carries none of the
+//                 restriction's code
+enum XROp { XR_FWD = 0, XR_INV_GAUGE = 1, XR_INV_REAL = 2, XR_INV_GAUGE_JET = 3 };
 
 template <int N, int G = 1, bool KM = false>
 struct XRShape {
@@ -216,8 +219,9 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
         }
         float* __restrict__ rout = a.rout + sim * a.bs_r;
         float4* __restrict__ psi = a.psi + sim * a.bs_psi;
-        const bool use_jet = a.use_jet != 0;
-        const JetArgs jet = a.jets ? a.jets[sim] : a.jet;
+        constexpr bool kJet = OP == XR_INV_GAUGE_JET;
+        JetArgs jet;
+        if constexpr (kJet) jet = a.jets ? a.jets[sim] : a.jet;
         auto src = [&](int j) -> T {
             const int k = j <= N / 2 ? j : N - j;
             float2 u, v;
@@ -238,11 +242,11 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
                 if (v0) rout[b0 + j] = v.x;
                 if (v1) rout[b1 + j] = v.y;
             } else {
-                static_assert(OP == XR_INV_GAUGE, "unhandled real x-pass op");
+                static_assert(OP == XR_INV_GAUGE || OP == XR_INV_GAUGE_JET, "unhandled real x-pass op");
                 // both rows' psi loaded before either is stored (two loads in flight)
                 float4 p0 = v0 ? psi[b0 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
                 float4 p1 = v1 ? psi[b1 + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-                if (use_jet) {
+                if constexpr (kJet) {
                     if (v0) restrict_cell(a.g, jet, j, (int)(r0 % ny), (int)(r0 / ny), b0 + j, p0);
                     if (v1) restrict_cell(a.g, jet, j, (int)((r0 + 1) % ny), (int)((r0 + 1) / ny), b1 + j, p1);
                 }

@@ -109,6 +109,7 @@ cudaError_t launch_xreal(int op, const XArgs& a, cudaStream_t s) {
     switch (op) {
         case XR_FWD: return launch_xr_op<XR_FWD>(a, s);
         case XR_INV_GAUGE: return launch_xr_op<XR_INV_GAUGE>(a, s);
+        case XR_INV_GAUGE_JET: return launch_xr_op<XR_INV_GAUGE_JET>(a, s);
         case XR_INV_REAL: return launch_xr_op<XR_INV_REAL>(a, s);
         default: return cudaErrorInvalidValue;
     }

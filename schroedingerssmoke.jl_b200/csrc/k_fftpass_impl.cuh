@@ -77,6 +77,7 @@ cudaError_t launch_yz_ng(const YZArgs& a, cudaStream_t s) {
     EXT template cudaError_t launch_x_ng<NN, X_PSI_INV_NORM, G>(const XArgs&, cudaStream_t);     \
     EXT template cudaError_t launch_xr_ng<NN, XR_FWD, G>(const XArgs&, cudaStream_t);            \
     EXT template cudaError_t launch_xr_ng<NN, XR_INV_GAUGE, G>(const XArgs&, cudaStream_t);      \
+    EXT template cudaError_t launch_xr_ng<NN, XR_INV_GAUGE_JET, G>(const XArgs&, cudaStream_t);  \
     EXT template cudaError_t launch_yz_ng<NN, float4, YZ_FWD, G>(const YZArgs&, cudaStream_t);   \
     EXT template cudaError_t launch_yz_ng<NN, float4, YZ_INV, G>(const YZArgs&, cudaStream_t);   \
     EXT template cudaError_t launch_yz_ng<NN, float4, YZ_MASK, G>(const YZArgs&, cudaStream_t);  \
@@ -86,7 +87,7 @@ cudaError_t launch_yz_ng(const YZArgs& a, cudaStream_t s) {
 
 // is the op one of the grouped ones (x pass / real x pass / y-z pass)?
 constexpr bool grouped_x_op(int op) { return op == X_PSI_FWD || op == X_PSI_INV_NORM; }
-constexpr bool grouped_xr_op(int op) { return op == XR_FWD || op == XR_INV_GAUGE; }
+constexpr bool grouped_xr_op(int op) { return op == XR_FWD || op == XR_INV_GAUGE || op == XR_INV_GAUGE_JET; }
 constexpr bool grouped_yz_op(int op, bool psi) { return psi ? (op == YZ_FWD || op == YZ_INV || op == YZ_MASK)
                                                             : (op == YZ_FWD || op == YZ_INV || op == YZ_FAC); }
 

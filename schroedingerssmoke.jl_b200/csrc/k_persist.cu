@@ -125,7 +125,12 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
             break;
         case PK_XR_INV_GAUGE:
             with_xlen(ph.len,
-                      [&](auto n) { xreal_body<decltype(n)::value, XR_INV_GAUGE, 1, true>(ph.x, bk, sm, bar); });
+                      [&](auto n) {
+                          if (ph.x.use_jet)
+                              xreal_body<decltype(n)::value, XR_INV_GAUGE_JET, 1, true>(ph.x, bk, sm, bar);
+                          else
+                              xreal_body<decltype(n)::value, XR_INV_GAUGE, 1, true>(ph.x, bk, sm, bar);
+                      });
             break;
         case PK_PLANE:
             with_plane(ph.len, [&](auto n) {
@@ -134,10 +139,13 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
             });
             break;
         case PK_DIV:
-            stencil_body<ST_DIV>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_DIV>*>(sm), bar);
+            if (ph.st.use_jet)
+                stencil_body<ST_DIV, true>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_DIV>*>(sm), bar);
+            else
+                stencil_body<ST_DIV, false>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_DIV>*>(sm), bar);
             break;
-        case PK_VEL:
-            stencil_body<ST_VEL>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
+        case PK_VEL:  // the one-form is never restricted (isf_batch.cu builds it with use_jet 0)
+            stencil_body<ST_VEL, false>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
             break;
         case PK_EMIT: {
             const long long j = (long long)bk.x * ph.vblk + vt;

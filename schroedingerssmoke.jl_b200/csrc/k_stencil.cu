@@ -4,11 +4,11 @@
 
 namespace isf {
 
-template <int OP>
+template <int OP, bool JET>
 __global__ void __launch_bounds__(st::BX* st::TY) k_stencil(StencilArgs a) {
     pdl_enter();
     __shared__ StencilSmem<OP> sm;
-    stencil_body<OP>(a, launch_blk(), sm);
+    stencil_body<OP, JET>(a, launch_blk(), sm);
 }
 
 cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
@@ -16,8 +16,14 @@ cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
     const int sz = op == ST_DIV ? st::planes_per_cta<ST_DIV>() : st::planes_per_cta<ST_VEL>();
     dim3 grid((unsigned)((a.g.n[0] + st::BX - 1) / st::BX), (unsigned)((a.g.n[1] + st::BY - 1) / st::BY),
               (unsigned)(((a.g.n[2] + sz - 1) / sz) * nsim));
-    if (op == ST_DIV) return launch_pdl(k_stencil<ST_DIV>, grid, dim3(st::BX * st::TY), 0, s, a);
-    if (op == ST_VEL) return launch_pdl(k_stencil<ST_VEL>, grid, dim3(st::BX * st::TY), 0, s, a);
+    const dim3 blk(st::BX * st::TY);
+    const bool jet = a.use_jet != 0;
+    if (op == ST_DIV)
+        return jet ? launch_pdl(k_stencil<ST_DIV, true>, grid, blk, 0, s, a)
+                   : launch_pdl(k_stencil<ST_DIV, false>, grid, blk, 0, s, a);
+    if (op == ST_VEL)
+        return jet ? launch_pdl(k_stencil<ST_VEL, true>, grid, blk, 0, s, a)
+                   : launch_pdl(k_stencil<ST_VEL, false>, grid, blk, 0, s, a);
     return cudaErrorInvalidValue;
 }
 
