@@ -69,7 +69,9 @@ struct XShape {
     static constexpr size_t SMEM = (size_t)G * N * C * sizeof(typename XTraits<OP>::T);
 };
 
-template <int N, int OP, int G, class BarT = CtaBar>
+// FULL: the launch has whole tiles only (the row count a multiple of C G), so
+// no pencil needs the past-the-end guard
+template <int N, int OP, int G, bool FULL = false, class BarT = CtaBar>
 __device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned char* smraw,
                                            const BarT& bar = BarT()) {
     using Tr = XTraits<OP>;
@@ -83,7 +85,7 @@ __device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned
     const long long rb = row * N;
     // the last CTA of a grid whose row count is not a multiple of C holds
     // pencils past the end: they read zeros and store nothing
-    const bool valid = row < (long long)a.g.n[1] * a.g.n[2];
+    const bool valid = FULL || row < (long long)a.g.n[1] * a.g.n[2];
     float4* __restrict__ psi = a.psi + bk.y * a.bs_psi;
     float2* __restrict__ F = a.F + bk.y * a.bs_F;
     T x[Plan<N>::EMAX];
@@ -110,11 +112,11 @@ __device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned
     Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst, bar);
 }
 
-template <int N, int OP, int G>
+template <int N, int OP, int G, bool FULL = false>
 __global__ void __launch_bounds__(XShape<N, OP, G>::BLK) k_xpass(XArgs a) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
-    xpass_body<N, OP, G>(a, launch_blk(), smraw);
+    xpass_body<N, OP, G, FULL>(a, launch_blk(), smraw);
 }
 
 // ------------------------------------------- x pass of real data (Poisson)
@@ -428,7 +430,8 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-template <int N, class T, int OP, int G, class BarT = CtaBar>
+// FULL: the row length is a multiple of C, so no column needs the past-the-end guard
+template <int N, class T, int OP, int G, bool FULL = false, class BarT = CtaBar>
 __device__ __forceinline__ void yzpass_body(const YZArgs a, const Blk bk, unsigned char* smraw,
                                             const BarT& bar = BarT()) {
     constexpr int C = YZShape<N, T>::C;
@@ -453,7 +456,7 @@ __device__ __forceinline__ void yzpass_body(const YZArgs a, const Blk bk, unsign
 
     // columns past the row's end (a row length that is not a multiple of
     // C) read zeros and store nothing
-    const bool valid = x0 + q < rl;
+    const bool valid = FULL || x0 + q < rl;
     auto gsrc = [&](int j) -> T { return valid ? data[base + j * stride + q] : T{}; };
     auto gdst = [&](int j, const T& v) {
         if (valid) data[base + j * stride + q] = v;
@@ -501,11 +504,11 @@ __device__ __forceinline__ void yzpass_body(const YZArgs a, const Blk bk, unsign
     }
 }
 
-template <int N, class T, int OP, int G>
+template <int N, class T, int OP, int G, bool FULL = false>
 __global__ void __launch_bounds__(YZShape<N, T, OP, G>::BLK, YZShape<N, T, OP, G>::MINB) k_yzpass(YZArgs a) {
     pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
-    yzpass_body<N, T, OP, G>(a, launch_blk(), smraw);
+    yzpass_body<N, T, OP, G, FULL>(a, launch_blk(), smraw);
 }
 
 }  // namespace isf

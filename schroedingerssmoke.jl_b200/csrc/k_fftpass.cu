@@ -29,32 +29,6 @@ bool grouped_tile_ok(int n, int groups) {
     return groups <= 1 || ((groups == 2 || groups == 4) && grouped_size(n));
 }
 
-#define ISF_SIZE_SWITCH(n, MACRO)                  \
-    switch (n) {                                   \
-        case 8: MACRO(8);                          \
-        case 12: MACRO(12);                        \
-        case 16: MACRO(16);                        \
-        case 24: MACRO(24);                        \
-        case 32: MACRO(32);                        \
-        case 48: MACRO(48);                        \
-        case 64: MACRO(64);                        \
-        case 96: MACRO(96);                        \
-        case 128: MACRO(128);                      \
-        case 192: MACRO(192);                      \
-        case 256: MACRO(256);                      \
-        case 384: MACRO(384);                      \
-        case 512: MACRO(512);                      \
-        case 20: MACRO(20);                        \
-        case 40: MACRO(40);                        \
-        case 50: MACRO(50);                        \
-        case 56: MACRO(56);                        \
-        case 80: MACRO(80);                        \
-        case 100: MACRO(100);                      \
-        case 112: MACRO(112);                      \
-        case 160: MACRO(160);                      \
-        case 200: MACRO(200);                      \
-        default: return cudaErrorInvalidValue;     \
-    }
 
 template <int N, int OP>
 static cudaError_t launch_x_n(const XArgs& a, cudaStream_t s) {
@@ -74,6 +48,9 @@ static cudaError_t launch_x_op(const XArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_xpass(int op, const XArgs& a, cudaStream_t s) {
+    const bool psi_op = op == X_PSI_FWD || op == X_PSI_INV || op == X_PSI_INV_NORM;
+    if (psi_op && a.groups <= 1 && ((long long)a.g.n[1] * a.g.n[2]) % XTraits<X_PSI_FWD>::C == 0)
+        return launch_xpass_full(op, a, s);
     switch (op) {
         case X_PSI_FWD: return launch_x_op<X_PSI_FWD>(a, s);
         case X_PSI_INV: return launch_x_op<X_PSI_INV>(a, s);
@@ -134,6 +111,7 @@ static cudaError_t launch_yz_op(const YZArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_yzpass_psi(int op, const YZArgs& a, cudaStream_t s) {
+    if (a.groups <= 1 && a.row % YZShape<8, float4>::C == 0) return launch_yzpass_psi_full(op, a, s);
     switch (op) {
         case YZ_FWD: return launch_yz_op<float4, YZ_FWD>(a, s);
         case YZ_INV: return launch_yz_op<float4, YZ_INV>(a, s);

@@ -33,17 +33,18 @@ cudaError_t ensure_smem(K kernel, size_t smem, std::atomic<unsigned long long>& 
 
 inline unsigned batch_dim(int nsim) { return (unsigned)(nsim > 1 ? nsim : 1); }
 
-template <int N, int OP, int G>
+template <int N, int OP, int G, bool FULL = false>
 cudaError_t launch_x_ng(const XArgs& a, cudaStream_t s) {
     using Sh = XShape<N, OP, G>;
     static std::atomic<unsigned long long> done{0};
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
-    // grouped tiles need whole tiles; single groups guard a partial last one
-    if (G > 1 && rows % (Sh::C * G) != 0) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_smem(k_xpass<N, OP, G>, Sh::SMEM, done);
+    // grouped tiles (and the FULL variant) need whole tiles; single groups
+    // guard a partial last one
+    if ((G > 1 || FULL) && rows % (Sh::C * G) != 0) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_smem(k_xpass<N, OP, G, FULL>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((rows + Sh::C * G - 1) / (Sh::C * G)), batch_dim(a.nsim));
-    return launch_pdl(k_xpass<N, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
+    return launch_pdl(k_xpass<N, OP, G, FULL>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 template <int N, int OP, int G, bool KM = false>
@@ -58,17 +59,51 @@ cudaError_t launch_xr_ng(const XArgs& a, cudaStream_t s) {
     return launch_pdl(k_xreal<N, OP, G, KM>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
-template <int N, class T, int OP, int G>
+template <int N, class T, int OP, int G, bool FULL = false>
 cudaError_t launch_yz_ng(const YZArgs& a, cudaStream_t s) {
     using Sh = YZShape<N, T, OP, G>;
     static std::atomic<unsigned long long> done{0};
     const int other = (a.axis == 1) ? a.g.n[2] : a.g.n[1];
-    if (other % G != 0 || (G > 1 && a.row % Sh::C != 0)) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_smem(k_yzpass<N, T, OP, G>, Sh::SMEM, done);
+    if (other % G != 0 || ((G > 1 || FULL) && a.row % Sh::C != 0)) return cudaErrorInvalidValue;
+    cudaError_t e = ensure_smem(k_yzpass<N, T, OP, G, FULL>, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((a.row + Sh::C - 1) / Sh::C), (unsigned)(other / G), batch_dim(a.nsim));
-    return launch_pdl(k_yzpass<N, T, OP, G>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
+    return launch_pdl(k_yzpass<N, T, OP, G, FULL>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
+
+// every supported pencil length, each case expanding MACRO(n)
+#define ISF_SIZE_SWITCH(n, MACRO)                  \
+    switch (n) {                                   \
+        case 8: MACRO(8);                          \
+        case 12: MACRO(12);                        \
+        case 16: MACRO(16);                        \
+        case 24: MACRO(24);                        \
+        case 32: MACRO(32);                        \
+        case 48: MACRO(48);                        \
+        case 64: MACRO(64);                        \
+        case 96: MACRO(96);                        \
+        case 128: MACRO(128);                      \
+        case 192: MACRO(192);                      \
+        case 256: MACRO(256);                      \
+        case 384: MACRO(384);                      \
+        case 512: MACRO(512);                      \
+        case 20: MACRO(20);                        \
+        case 40: MACRO(40);                        \
+        case 50: MACRO(50);                        \
+        case 56: MACRO(56);                        \
+        case 80: MACRO(80);                        \
+        case 100: MACRO(100);                      \
+        case 112: MACRO(112);                      \
+        case 160: MACRO(160);                      \
+        case 200: MACRO(200);                      \
+        default: return cudaErrorInvalidValue;     \
+    }
+
+// whole-tile launchers of the psi passes (k_fftpass_full.cu): the x passes
+// X_PSI_* with the row count a multiple of 8, the y / z passes YZ_FWD /
+// YZ_INV / YZ_MASK on float4 with the row length a multiple of 8
+cudaError_t launch_xpass_full(int op, const XArgs& a, cudaStream_t s);
+cudaError_t launch_yzpass_psi_full(int op, const YZArgs& a, cudaStream_t s);
 
 // the grouped instantiations compiled in k_fftpass_g2.cu / k_fftpass_g4.cu:
 // the ops the batch runs (EXT is empty there and `extern` in k_fftpass.cu)

@@ -1,6 +1,7 @@
 // Particle kernels: seeded emission (add_particles!) and RK4 advection on the
 // staggered velocity (staggered_advect!).
 #include <cstdlib>
+#include <type_traits>
 
 #include "isf_launch.h"
 #include "isf_particles.cuh"
@@ -61,7 +62,7 @@ __global__ void k_emit_soa(float* __restrict__ x, float* __restrict__ y, float* 
 #else
 #define ISF_ADV_BOUNDS __launch_bounds__(256)
 #endif
-template <bool POW2, bool NORMW, bool FIDX>
+template <bool POW2, bool NORMW, bool FIDX, bool ORD>
 __global__ void ISF_ADV_BOUNDS k_advect(Grid g, float* __restrict__ parts, int np,
                                                 const float* __restrict__ vel,
                                                 unsigned long long* __restrict__ counters, long long bs_vel,
@@ -75,7 +76,7 @@ __global__ void ISF_ADV_BOUNDS k_advect(Grid g, float* __restrict__ parts, int n
     unsigned long long* chk = counters ? counters + 2 : nullptr;  // ISF_CHECK records
     const float dt = g.dt, s6 = g.dt / 6.0f;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < np; t += gridDim.x * blockDim.x)
-        advect_slot<POW2, NORMW, CtaBar, FIDX>(kc, parts, order ? __ldg(order + t) : t, dt, s6, clamps, live, chk);
+        advect_slot<POW2, NORMW, CtaBar, FIDX>(kc, parts, ORD ? __ldg(order + t) : t, dt, s6, clamps, live, chk);
     if (counters) {
         // block-aggregated counters: one atomic per CTA and counter
         __shared__ unsigned red[2][8];
@@ -517,7 +518,8 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
         int dev = 0, sms = 0, per = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false, false, true>, blk, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advect<false, false, true, false>, blk, 0) !=
+                cudaSuccess ||
             per < 1)
             return cudaErrorInvalidValue;
         resident = sms * per;
@@ -534,12 +536,17 @@ cudaError_t launch_advect(const Grid& g, float* parts, long long np, const float
     auto go = [&](auto kernel) {
         return launch_pdl(kernel, grid, dim3(blk), 0, s, g, parts, (int)np, vel, counters, bs_vel, order);
     };
-    if (g.norm_w) {
-        if (pow2) return fidx ? go(k_advect<true, true, true>) : go(k_advect<true, true, false>);
-        return fidx ? go(k_advect<false, true, true>) : go(k_advect<false, true, false>);
-    }
-    if (pow2) return fidx ? go(k_advect<true, false, true>) : go(k_advect<true, false, false>);
-    return fidx ? go(k_advect<false, false, true>) : go(k_advect<false, false, false>);
+    // the traversal through a slot permutation is its own instantiation, so
+    // the storage-order loop carries no test of it
+    auto pick = [&](auto p2, auto nw) {
+        constexpr bool P2 = decltype(p2)::value, NW = decltype(nw)::value;
+        if (order) return fidx ? go(k_advect<P2, NW, true, true>) : go(k_advect<P2, NW, false, true>);
+        return fidx ? go(k_advect<P2, NW, true, false>) : go(k_advect<P2, NW, false, false>);
+    };
+    using T = std::true_type;
+    using F = std::false_type;
+    if (g.norm_w) return pow2 ? pick(T(), T()) : pick(F(), T());
+    return pow2 ? pick(T(), F()) : pick(F(), F());
 }
 
 cudaError_t launch_order_count(const Grid& g, const float* parts, long long np, const OrderBufs& b, cudaStream_t s) {

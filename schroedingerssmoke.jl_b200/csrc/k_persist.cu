@@ -84,7 +84,9 @@ __device__ bool wait_groups(const PPlan& P, const PPhase& q, int step, int nsg, 
     return true;
 }
 
-// one tile (virtual CTA) of a phase
+// one tile (virtual CTA) of a phase; the persistent grids have whole tiles
+// only (nx and ny = nz multiples of 8), so the passes take their
+// whole-tile variants
 __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int tile, int step, int vt,
                                          unsigned char* sm, const NamedBar& bar) {
     Blk bk;
@@ -106,19 +108,19 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
             break;
         }
         case PK_X_FWD:
-            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_FWD, 1>(ph.x, bk, sm, bar); });
+            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_FWD, 1, true>(ph.x, bk, sm, bar); });
             break;
         case PK_X_INV_NORM:
-            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_INV_NORM, 1>(ph.x, bk, sm, bar); });
+            with_xlen(ph.len, [&](auto n) { xpass_body<decltype(n)::value, X_PSI_INV_NORM, 1, true>(ph.x, bk, sm, bar); });
             break;
         case PK_Y_FWD:
-            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_FWD, 1>(ph.yz, bk, sm, bar); });
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_FWD, 1, true>(ph.yz, bk, sm, bar); });
             break;
         case PK_Z_MASK:
-            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_MASK, 1>(ph.yz, bk, sm, bar); });
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_MASK, 1, true>(ph.yz, bk, sm, bar); });
             break;
         case PK_Y_INV:
-            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_INV, 1>(ph.yz, bk, sm, bar); });
+            with_plane(ph.len, [&](auto n) { yzpass_body<decltype(n)::value, float4, YZ_INV, 1, true>(ph.yz, bk, sm, bar); });
             break;
         case PK_XR_FWD:
             with_xlen(ph.len, [&](auto n) { xreal_body<decltype(n)::value, XR_FWD, 1, true>(ph.x, bk, sm, bar); });
