@@ -56,8 +56,9 @@ struct StencilSmem<ST_VEL> {
 // JET: psi is restricted in the nozzle on the fly (a.use_jet set).  A
 // compile-time switch: left to a run-time test, the restriction's code shaped
 // the plane loop of every launch (about 24 instructions per cell more, with
-// use_jet 0).
-template <int OP, bool JET, class B = CtaBar>
+// use_jet 0).  SHARP (one-form stencil): the one-form is divided by the cell
+// sizes (a.sharp set), also a compile-time switch.
+template <int OP, bool JET, bool SHARP = false, class B = CtaBar>
 __device__ __forceinline__ void stencil_body(const StencilArgs a, const Blk bk, StencilSmem<OP>& S,
                                              const B& bar = B()) {
     using namespace st;
@@ -105,7 +106,6 @@ __device__ __forceinline__ void stencil_body(const StencilArgs a, const Blk bk, 
     if constexpr (JET) jet = a.jets ? a.jets[sim] : a.jet;
     const float id0 = g.inv_d2[0], id1 = g.inv_d2[1], id2 = g.inv_d2[2];
     const float hb = a.hbar;
-    const bool sharp = a.sharp != 0;
     const float di0 = g.dinv[0], di1 = g.dinv[1], di2 = g.dinv[2];
     const int pnx = g.pnx, pnxy = g.pnxy;
     float4* __restrict__ out4 = reinterpret_cast<float4*>(out);
@@ -209,7 +209,7 @@ __device__ __forceinline__ void stencil_body(const StencilArgs a, const Blk bk, 
                     float ax = pair_angle(c0, tile[cur][r + 1][tx + 2]) * hb;
                     float ay = pair_angle(c0, tile[cur][r + 2][tx + 1]) * hb;
                     float az = pair_angle(c0, tile[nxt][r + 1][tx + 1]) * hb;
-                    if (sharp) {
+                    if constexpr (SHARP) {
                         ax = __fmul_rn(ax, di0);
                         ay = __fmul_rn(ay, di1);
                         az = __fmul_rn(az, di2);

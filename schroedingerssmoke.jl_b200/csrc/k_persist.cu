@@ -147,7 +147,10 @@ __device__ __forceinline__ void run_tile(const PPlan& P, const PPhase& ph, int t
                 stencil_body<ST_DIV, false>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_DIV>*>(sm), bar);
             break;
         case PK_VEL:  // the one-form is never restricted (isf_batch.cu builds it with use_jet 0)
-            stencil_body<ST_VEL, false>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
+            if (ph.st.sharp)
+                stencil_body<ST_VEL, false, true>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
+            else
+                stencil_body<ST_VEL, false>(ph.st, bk, *reinterpret_cast<StencilSmem<ST_VEL>*>(sm), bar);
             break;
         case PK_EMIT: {
             const long long j = (long long)bk.x * ph.vblk + vt;

@@ -4,11 +4,11 @@
 
 namespace isf {
 
-template <int OP, bool JET>
+template <int OP, bool JET, bool SHARP = false>
 __global__ void __launch_bounds__(st::BX* st::TY) k_stencil(StencilArgs a) {
     pdl_enter();
     __shared__ StencilSmem<OP> sm;
-    stencil_body<OP, JET>(a, launch_blk(), sm);
+    stencil_body<OP, JET, SHARP>(a, launch_blk(), sm);
 }
 
 cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
@@ -21,9 +21,13 @@ cudaError_t launch_stencil(int op, const StencilArgs& a, cudaStream_t s) {
     if (op == ST_DIV)
         return jet ? launch_pdl(k_stencil<ST_DIV, true>, grid, blk, 0, s, a)
                    : launch_pdl(k_stencil<ST_DIV, false>, grid, blk, 0, s, a);
-    if (op == ST_VEL)
+    if (op == ST_VEL) {
+        if (a.sharp)
+            return jet ? launch_pdl(k_stencil<ST_VEL, true, true>, grid, blk, 0, s, a)
+                       : launch_pdl(k_stencil<ST_VEL, false, true>, grid, blk, 0, s, a);
         return jet ? launch_pdl(k_stencil<ST_VEL, true>, grid, blk, 0, s, a)
                    : launch_pdl(k_stencil<ST_VEL, false>, grid, blk, 0, s, a);
+    }
     return cudaErrorInvalidValue;
 }
 
