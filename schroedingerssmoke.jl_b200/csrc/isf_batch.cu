@@ -26,6 +26,7 @@
 #include "isf_launch.h"
 #include "isf_passes.cuh"
 #include "isf_persist.h"
+#include "isf_stencil.cuh"
 
 namespace isf {
 namespace {
@@ -461,7 +462,7 @@ bool class_chain(const isf_batch* b, const BatchClass& c, int ci, std::vector<PP
     yzphase(PK_Y_INV, 1);
     xphase(PK_X_INV_NORM);
     auto projection = [&](const JetArgs* jets) {
-        PPhase d = new_phase(c, ci, PK_DIV, 0, up(nx, 32), up(ny, 16), up(nz, 8) * ns);
+        PPhase d = new_phase(c, ci, PK_DIV, 0, up(nx, st::BX), up(ny, st::BY), up(nz, st::planes_per_cta<ST_DIV>()) * ns);
         d.st = bst(c, c.f, c.g.N);
         PPhase f = new_phase(c, ci, PK_XR_FWD, nx, rows / 32, ns, 1);
         f.x = bx(c, 1);
@@ -493,7 +494,7 @@ bool class_chain(const isf_batch* b, const BatchClass& c, int ci, std::vector<PP
         }
         projection(b->jets + c.first);
     }
-    PPhase v = new_phase(c, ci, PK_VEL, 0, up(nx, 32), up(ny, 16), up(nz, 4) * ns);
+    PPhase v = new_phase(c, ci, PK_VEL, 0, up(nx, st::BX), up(ny, st::BY), up(nz, st::planes_per_cta<ST_VEL>()) * ns);
     v.st = bst(c, c.vel, kVelComp * c.g.NP);
     v.st.hbar = c.g.hbar;
     v.st.sharp = 1;
