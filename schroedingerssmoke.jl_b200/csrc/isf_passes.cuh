@@ -318,6 +318,9 @@ __device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsi
     float2* __restrict__ Fp = a.F + bk.y * a.bs_F + (long long)kx * N * N;
     float2 x[PlanPlane<N>::EMAX];
     const float2 zero = make_float2(0.f, 0.f);
+    // every group's pencils exist in every round when the groups divide the
+    // pencils evenly (N = 128: 4 groups, 2 rounds): no guard is compiled then
+    constexpr bool kAllOn = (N / C) % Sh::GROUPS == 0;
     // y transforms: pencil = row z of the plane, lanes along y.  The forward
     // one reads its rows straight from HBM into registers and leaves them in
     // shared memory; the inverse one reads shared memory and writes HBM.
@@ -327,7 +330,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsi
 #pragma unroll 1
         for (int round = 0; round < Sh::ROUNDS; ++round) {
             const int z = (round * Sh::GROUPS + grp) * C + q;
-            const bool on = z < N;
+            const bool on = kAllOn || z < N;
             auto src = [&](int j) -> float2 {
                 if (S < 0) return on ? Fp[z * N + j] : zero;
                 return on ? plane[z * N + j] : zero;
@@ -353,7 +356,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsi
 #pragma unroll 1
         for (int round = 0; round < Sh::ROUNDS; ++round) {
             const int ky = (round * Sh::GROUPS + grp) * C + q;
-            const bool on = ky < N;
+            const bool on = kAllOn || ky < N;
             const int kyc = on ? ky : 0;
             const double dxo = sx + a.g.s2[1][kyc];
             const bool zero_line = (kx == 0) && (kyc == 0);
