@@ -426,7 +426,9 @@ struct YZShape {
     static constexpr size_t SMEM = (size_t)G * N * C * sizeof(T);
     static constexpr int MINT = (OP < 2) ? ISF_YZ_MIN_THREADS
                                 : (sizeof(T) == 16 ? ISF_YZ_PSI_SPECTRAL_MIN_THREADS : ISF_YZ_SPECTRAL_MIN_THREADS);
-    static constexpr int MINB = (MINT / BLK) > 1 ? (MINT / BLK) : 1;
+    // at least 1, at most the 32 resident CTAs an SM takes (short pencils
+    // make small CTAs)
+    static constexpr int MINB = (MINT / BLK) > 32 ? 32 : ((MINT / BLK) > 1 ? (MINT / BLK) : 1);
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
