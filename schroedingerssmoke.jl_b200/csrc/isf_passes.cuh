@@ -269,6 +269,17 @@ __global__ void __launch_bounds__(XRShape<N, G, KM>::BLK) k_xreal(XArgs a) {
     xreal_body<N, OP, G, KM>(a, launch_blk(), smraw);
 }
 
+// The same pass compiled for 3 resident CTAs per SM (at most 42 registers),
+// launched for rows of at least 256 cells: the gauge pass at 256x128x128 ran
+// 35.4 -> 34.6 us.  The ensembles' short rows keep k_xreal; capped, their
+// batched step was 5 % slower.
+template <int N, int OP, int G, bool KM = false>
+__global__ void __launch_bounds__(XRShape<N, G, KM>::BLK, 3) k_xreal_long(XArgs a) {
+    pdl_enter();
+    extern __shared__ __align__(16) unsigned char smraw[];
+    xreal_body<N, OP, G, KM>(a, launch_blk(), smraw);
+}
+
 // ------------------------------------------- Poisson solve on (y, z) planes
 // With the k-major half spectrum, the y and z transforms of one kx are a
 // contiguous N x N plane (ny = nz = N).  One CTA holds the plane in shared

@@ -53,10 +53,14 @@ cudaError_t launch_xr_ng(const XArgs& a, cudaStream_t s) {
     static std::atomic<unsigned long long> done{0};
     const long long rows = (long long)a.g.n[1] * a.g.n[2];
     if ((G > 1 || KM) && rows % (2 * Sh::C * G) != 0) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_smem(k_xreal<N, OP, G, KM>, Sh::SMEM, done);
+    constexpr auto kern = [] {
+        if constexpr (N >= 256) return k_xreal_long<N, OP, G, KM>;
+        else return k_xreal<N, OP, G, KM>;
+    }();
+    cudaError_t e = ensure_smem(kern, Sh::SMEM, done);
     if (e != cudaSuccess) return e;
     const dim3 grid((unsigned)((rows + 2 * Sh::C * G - 1) / (2 * Sh::C * G)), batch_dim(a.nsim));
-    return launch_pdl(k_xreal<N, OP, G, KM>, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
+    return launch_pdl(kern, grid, dim3(Sh::BLK), Sh::SMEM, s, a);
 }
 
 template <int N, class T, int OP, int G, bool FULL = false>
