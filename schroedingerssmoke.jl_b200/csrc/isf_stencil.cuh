@@ -20,13 +20,14 @@ namespace isf {
 
 namespace st {
 
-// z planes per CTA: the div stencil (which also computes the tile's halo
-// angles) amortises its prologue over more planes than the one-form stencil
+// z planes per CTA (both stencils: at 256x128x128 the div stencil ran 39.8
+// us over 4 planes and 37.3 over 8; the one-form stencil 36.3 over 4 and
+// 35.9 over 8)
 #ifndef ISF_ST_SZ
 #define ISF_ST_SZ 8
 #endif
 #ifndef ISF_ST_SZ_VEL
-#define ISF_ST_SZ_VEL 4
+#define ISF_ST_SZ_VEL 8
 #endif
 #ifndef ISF_ST_RPT
 #define ISF_ST_RPT 2
