@@ -84,15 +84,38 @@ __device__ __forceinline__ void pdl_enter() {
 // kernel launched on its own (CtaBar), or the named barrier of one virtual
 // CTA, n threads of a larger block, in the persistent batch kernel
 // (NamedBar; ids 1..15, n a multiple of 32).
+// xsync() orders the exchanges between FFT stages (isf_fft.cuh); for
+// these two it is the same barrier as sync().
 struct CtaBar {
     static constexpr bool kLaunch = true;
     __device__ __forceinline__ void sync() const { __syncthreads(); }
+    __device__ __forceinline__ void xsync() const { __syncthreads(); }
 };
 struct NamedBar {
     static constexpr bool kLaunch = false;
     int id, n;
     __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+    __device__ __forceinline__ void xsync() const { sync(); }
 };
+
+// The barriers of a pass whose every pencil is held by lanes of one warp
+// (NT lanes per pencil with NT dividing 32, the C pencils of a group laid
+// out lane after lane from a warp boundary).  An exchange between FFT stages
+// writes and reads only its own pencil's slots of the shared tile, so it
+// orders the warp (__syncwarp); sync() stays the barrier of the whole
+// (virtual) CTA for the steps that share the tile across pencils.
+template <class B>
+struct WarpXBar {
+    static constexpr bool kLaunch = B::kLaunch;
+    B b;
+    __device__ __forceinline__ void sync() const { b.sync(); }
+    __device__ __forceinline__ void xsync() const { __syncwarp(); }
+};
+template <int NT, int C, class B>
+__device__ __forceinline__ auto pencil_bar(const B& b) {
+    if constexpr (NT <= 32 && 32 % NT == 0 && (NT * C) % 32 == 0) return WarpXBar<B>{b};
+    else return b;
+}
 
 // Block coordinates and thread index of one (virtual) CTA: blockIdx /
 // threadIdx for a kernel launched on its own, the work item's in the

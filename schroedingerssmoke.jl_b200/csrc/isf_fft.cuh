@@ -259,10 +259,10 @@ __device__ __forceinline__ void pipeline(T* x, int t, int q, T* sm, const float2
         scatter<N, NT, R, P>(x, t, dst);
     } else {
         scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
-        bar.sync();
+        bar.xsync();
         constexpr int R2 = First<Rest...>::value;
         gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
-        bar.sync();
+        bar.xsync();
         pipeline<N, NT, C, S, T, Dst, B, P * R, Rest...>(x, t, q, sm, tw, dst, bar);
     }
 }
@@ -277,10 +277,10 @@ __device__ __forceinline__ void pipeline_keep(T* x, int t, int q, T* sm, const f
     butterflies<N, NT, R, P, S>(x, t, tw);
     if constexpr (sizeof...(Rest) > 0) {
         scatter<N, NT, R, P>(x, t, [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; });
-        bar.sync();
+        bar.xsync();
         constexpr int R2 = First<Rest...>::value;
         gather<N, NT, R2>(x, t, [&](int j) { return sm[sidx<C>(j, q)]; });
-        bar.sync();
+        bar.xsync();
         pipeline_keep<N, NT, C, S, T, B, P * R, Rest...>(x, t, q, sm, tw, bar);
     }
 }

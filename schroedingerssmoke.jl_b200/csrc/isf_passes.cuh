@@ -109,7 +109,7 @@ __device__ __forceinline__ void xpass_body(const XArgs a, const Blk bk, unsigned
             F[rb + j] = v;
         }
     };
-    Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst, bar);
+    Plan<N>::template run<C, Tr::S, false>(x, t, q, sm, a.g.tw[0], src, dst, pencil_bar<NT, C>(bar));
 }
 
 template <int N, int OP, int G, bool FULL = false>
@@ -177,7 +177,7 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
             return make_float2(v0 ? ldm<BarT>(&f0[j]) : 0.f, v1 ? ldm<BarT>(&f1[j]) : 0.f);
         };
         auto sdst = [&](int j, const T& v) { sm[sidx<C>(j, q)] = v; };
-        Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst, bar);
+        Plan<N>::template run<C, -1, false>(x, t, q, sm, a.g.tw[0], src, sdst, pencil_bar<NT, C>(bar));
         bar.sync();
         if constexpr (KM) {
             // lanes over the row pairs of the group: 16 x 16 B per k
@@ -258,7 +258,7 @@ __device__ __forceinline__ void xreal_body(const XArgs a, const Blk bk, unsigned
         };
         // k-major: the staging aliases the tile, so the first gather must
         // complete before the first stage writes the tile
-        Plan<N>::template run<C, +1, KM>(x, t, q, sm, a.g.tw[0], src, dst, bar);
+        Plan<N>::template run<C, +1, KM>(x, t, q, sm, a.g.tw[0], src, dst, pencil_bar<NT, C>(bar));
     }
 }
 
