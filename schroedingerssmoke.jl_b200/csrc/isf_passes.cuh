@@ -334,7 +334,10 @@ __device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsi
     constexpr bool kAllOn = (N / C) % Sh::GROUPS == 0;
     // y transforms: pencil = row z of the plane, lanes along y.  The forward
     // one reads its rows straight from HBM into registers and leaves them in
-    // shared memory; the inverse one reads shared memory and writes HBM.
+    // shared memory; the inverse one reads shared memory and writes HBM.  A
+    // pencil's lanes are consecutive, so where they fit in one warp its stage
+    // exchanges are ordered by the warp (pencil_bar); the z transforms'
+    // lanes run across pencils and keep the CTA barrier.
     auto ysweep = [&](auto sign) {
         constexpr int S = decltype(sign)::value;
         const int t = lt % NT, q = lt / NT;
@@ -353,7 +356,7 @@ __device__ __forceinline__ void plane_body(const PlaneArgs a, const Blk bk, unsi
                 else
                     Fp[z * N + j] = v;
             };
-            PlanPlane<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst, bar);
+            PlanPlane<N>::template run<C, S, false>(x, t, q, tile, a.g.tw[1], src, dst, pencil_bar<NT, C>(bar));
             bar.sync();
         }
     };
