@@ -5,16 +5,18 @@
 
 namespace isf {
 
+// Both stencils are compiled for 4 resident CTAs per SM (at most 64
+// registers).  The one-form stencil: 60 registers and 185 instructions per
+// cell left to ptxas (35.9 us at 256x128x128), 64 and 181 capped (34.6 us).
 template <int OP, bool JET, bool SHARP = false>
-__global__ void __launch_bounds__(st::BX* st::TY) k_stencil(StencilArgs a) {
+__global__ void __launch_bounds__(st::BX* st::TY, 4) k_stencil(StencilArgs a) {
     pdl_enter();
     __shared__ StencilSmem<OP> sm;
     stencil_body<OP, JET, SHARP>(a, launch_blk(), sm);
 }
 
-// The div stencil compiled for 4 resident CTAs per SM: left to ptxas it
-// takes 48 registers and 235 instructions per cell (40.9 us at 256x128x128);
-// capped at 64 it runs 200 instructions per cell (37.9 us).
+// The div stencil: 48 registers and 235 instructions per cell left to
+// ptxas (40.9 us at 256x128x128), 64 and 200 capped (37.9 us).
 template <bool JET>
 __global__ void __launch_bounds__(st::BX* st::TY, 4) k_stencil_div(StencilArgs a) {
     pdl_enter();
