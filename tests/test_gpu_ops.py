@@ -36,7 +36,10 @@ def host(t):
 
 @pytest.mark.parametrize("dims", [(16, 8, 8), (32, 12, 24), (48, 32, 32), (96, 48, 48), (256, 128, 128),
                                   (512, 16, 8), (384, 8, 16), (192, 64, 8), (80, 40, 40), (100, 50, 50),
-                                  (56, 112, 20), (200, 50, 160)])
+                                  (56, 112, 20), (200, 50, 160),
+                                  # x rows whose pencils share a warp (16 and 8 lanes each), and a
+                                  # row of 8 whose pencils are single lanes
+                                  (128, 16, 8), (64, 8, 16), (8, 16, 32)])
 def test_fft3_matches_numpy(isfpkg, dims):
     isf = isfpkg.ISF((1, 1, 1), dims, HBAR, DT)
     rng = np.random.default_rng(1)
